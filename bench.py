@@ -1,0 +1,500 @@
+#!/usr/bin/env python
+"""The particle-grid hot path on B200: markers/s of the 3D quadratic gather + scatter.
+
+Workload (the configuration the metric is quoted on): a 256^3 periodic grid on the unit
+cube, QUADRATIC weights, float64; a 3-component field, each component a sum of 8
+Fourier modes cos(2 pi k.x + phi) with integer wave-vector components k_d in 1..8 and
+unit amplitude (seeded); N = 2^26 markers, 80% uniform in the cube and 20% in a
+Gaussian beam (sigma 0.05, centre 0.5, wrapped into the cube), in random order; marker
+weights uniform in [0.5, 1.5]. All inputs are synthetic (there is no dataset).
+
+One step, on markers in arbitrary order, results returned in that order:
+  sort the markers by cell tile (keys, stable radix sort), permute positions and
+  weights into tile order, gather E (3, N) from the field, scatter the weights into a
+  zeroed 1-component density, and return E to the markers' own order.
+`value` is N / step time with every input resident in HBM. `steady_state` times the
+gather + scatter alone on markers already in tile order (a PIC marker store kept
+sorted). `e2e` adds, every step, the host-to-device copy of positions and weights from
+pinned host memory and the device-to-host copy of E and the density. The positions
+alone (1.6 GB) exceed the 126 MB L2, so no flush is needed between steps.
+
+With --impl reference the same metric is measured on the reference's CPU
+implementation (the OpenMP restatement of its Pyccel kernels, oracle/cpu_baseline.c,
+with all host threads) on a bounded sample of the workload per step.
+
+Under torchrun (N GPUs) every rank runs the same workload on its own GPU (replicas: the
+hot path has no cross-GPU step on one grid); the time is the max over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+import torch
+
+ROOT = Path(__file__).resolve().parent
+if str(ROOT) not in sys.path:
+    sys.path.insert(0, str(ROOT))
+
+METRIC = "markers/s: 3D quadratic gather/scatter"
+GRID = 256
+TILE = (8, 8, 8)
+PEAK_FALLBACK_GBS = 6650.0
+
+
+def parse() -> argparse.Namespace:
+    p = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    p.add_argument("--markers", type=int, default=1 << 26)
+    p.add_argument("--dtype", choices=("f64", "f32"), default="f64")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-ref-cuda", action="store_true")
+    return p.parse_args()
+
+
+# ------------------------------------------------------------------ workload --
+
+
+def geometry() -> tuple:
+    h = 1.0 / GRID
+    return (0.0, 0.0, 0.0, h, h, h, GRID, GRID, GRID, 1, 1, 1)
+
+
+def make_field(device, dtype, seed: int = 0) -> torch.Tensor:
+    """(256, 256, 256, 3): per component a sum of 8 unit Fourier modes, k_d in 1..8."""
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    x = torch.arange(GRID, dtype=torch.float64, device=device) / GRID
+    field = torch.zeros((GRID, GRID, GRID, 3), dtype=torch.float64, device=device)
+    for c in range(3):
+        for _ in range(8):
+            k = torch.randint(1, 9, (3,), generator=g).tolist()
+            phi = float(torch.rand((), generator=g, dtype=torch.float64)) * 2 * np.pi
+            phase = 2 * np.pi * (k[0] * x[:, None, None] + k[1] * x[None, :, None] + k[2] * x[None, None, :])
+            field[..., c] += torch.cos(phase + phi)
+    return field.to(dtype)
+
+
+def make_markers(n: int, device, dtype, seed: int = 1) -> tuple[torch.Tensor, torch.Tensor]:
+    """Positions (3, n) -- 80% uniform, 20% beam N(0.5, 0.05) wrapped -- and weights (1, n)."""
+    g = torch.Generator(device=device).manual_seed(seed)
+    pos = torch.rand((3, n), generator=g, dtype=torch.float64, device=device)
+    beam = torch.rand(n, generator=g, dtype=torch.float64, device=device) < 0.2
+    gauss = 0.5 + 0.05 * torch.randn((3, n), generator=g, dtype=torch.float64, device=device)
+    pos = torch.where(beam[None, :], torch.remainder(gauss, 1.0), pos)
+    weights = 0.5 + torch.rand((1, n), generator=g, dtype=torch.float64, device=device)
+    return pos.to(dtype).contiguous(), weights.to(dtype).contiguous()
+
+
+def algorithmic_bytes(n: int, itemsize: int) -> dict[str, int]:
+    """Compulsory traffic: gather N (3 pos + 3 out) + field; scatter N (3 pos + 1 w) + 2 x density."""
+    nodes = GRID ** 3
+    return {
+        "gather": n * 6 * itemsize + nodes * 3 * itemsize,
+        "scatter": n * 4 * itemsize + nodes * 2 * itemsize,
+    }
+
+
+# -------------------------------------------------------------- clock samples --
+
+
+class ClockSampler:
+    """nvidia-smi clock and throttle samples of one GPU during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int) -> None:
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.index)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def _read(self) -> None:
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc) -> None:
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict | None:
+        rows = [line.split(", ") for line in self.lines if line.count(",") >= 8]
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        maxsm = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].strip().lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(maxsm) if maxsm else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# -------------------------------------------------------------------- helpers --
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        backend = "nccl" if torch.cuda.is_available() and args.impl == "ours" else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(local)
+    return world, rank, local
+
+
+def max_over_ranks(value: float, world: int, device) -> float:
+    if world == 1:
+        return value
+    import torch.distributed as dist
+
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int) -> None:
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def read_peak() -> tuple[float, str]:
+    path = ROOT / "MEASURED_PEAKS.json"
+    try:
+        peaks = json.loads(path.read_text())
+        return float(peaks["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return PEAK_FALLBACK_GBS, "fallback"
+
+
+def read_traffic(key: str) -> int | None:
+    """DRAM bytes per launch of a kernel from the committed ncu summary, if present."""
+    path = ROOT / "profiles" / "traffic.txt"
+    try:
+        for line in path.read_text().splitlines():
+            parts = line.split()
+            if len(parts) >= 2 and parts[0] == key:
+                return int(float(parts[1]))
+    except OSError:
+        pass
+    return None
+
+
+# ----------------------------------------------------------------- our step --
+
+
+class Step:
+    """The hot path on one GPU: sort, permute, gather, scatter, unpermute."""
+
+    def __init__(self, n: int, device, dtype) -> None:
+        import mpifield_b200 as mf
+        from mpifield_b200 import _lib
+
+        self.mf, self.lib = mf, _lib
+        self.n, self.device, self.dtype = n, device, dtype
+        self.geom = geometry()
+        self.field = make_field(device, dtype)
+        self.density = torch.zeros((GRID, GRID, GRID, 1), dtype=dtype, device=device)
+        self.E = torch.empty((3, n), dtype=dtype, device=device)
+        self.E_out = torch.empty((3, n), dtype=dtype, device=device)
+        self.kernels = (mf.KERNELS["gather_quadratic_3d"], mf.KERNELS["scatter_quadratic_3d"])
+
+    def sort(self, pos, w):
+        t = self.mf.sort_by_tile(pos, self.mf.QUADRATIC, self.geom, TILE)
+        return t, self.mf.permute(pos, t.order), self.mf.permute(w, t.order)
+
+    def gather_scatter(self, pos, w, events=None):
+        gather, scatter = self.kernels
+        if events is not None:
+            events[0].record()
+        gather(pos, self.field, self.E, *self.geom)
+        if events is not None:
+            events[1].record()
+        self.density.zero_()
+        scatter(pos, w, self.density, *self.geom)
+        if events is not None:
+            events[2].record()
+
+    def full(self, pos, w, events=None):
+        t, ps, ws = self.sort(pos, w)
+        self.gather_scatter(ps, ws, events)
+        self.mf.unpermute(self.E, t.order, out=self.E_out)
+
+
+def time_loop(fn, steps: int, warmup: int, world: int, device) -> float:
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record()
+    for _ in range(steps):
+        fn()
+    stop.record()
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    return max_over_ranks(start.elapsed_time(stop) / 1000.0, world, device)
+
+
+def ref_cuda_time(pos, w, field, density, E, steps: int) -> dict | None:
+    """The reference's CUDA gather_quadratic_3d + scatter_quadratic_3d (one thread per
+    marker, block 256), compiled for sm_100a from the reference sources (oracle/_ref)."""
+    import ctypes as C
+
+    path = ROOT / "oracle" / "_ref" / "libref_cuda.so"
+    if not path.exists():
+        return None
+    lib = C.CDLL(str(path))
+    n = pos.shape[1]
+    stream = torch.cuda.current_stream().cuda_stream
+
+    def view(t):
+        shape = (C.c_longlong * t.dim())(*t.shape)
+        strides = (C.c_longlong * t.dim())(*t.stride())
+        return [C.c_void_p(t.data_ptr()), shape, strides]
+
+    h = 1.0 / GRID
+    scal = [C.c_double(0.0)] * 3 + [C.c_double(h)] * 3 + [C.c_int(GRID)] * 3 + [C.c_int(1)] * 3
+    head = [C.c_longlong(n), C.c_int(256), C.c_int(0), C.c_void_p(stream)]
+    g_args = head + view(pos) + view(field) + view(E) + scal
+    s_args = head + view(pos) + view(w) + view(density) + scal
+
+    def step():
+        lib.refcuda_gather_quadratic_3d(*g_args)
+        density.zero_()
+        lib.refcuda_scatter_quadratic_3d(*s_args)
+
+    step()
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    g_ms, s_ms = 0.0, 0.0
+    for _ in range(steps):
+        ev[0].record()
+        lib.refcuda_gather_quadratic_3d(*g_args)
+        ev[1].record()
+        density.zero_()
+        lib.refcuda_scatter_quadratic_3d(*s_args)
+        ev[2].record()
+        torch.cuda.synchronize()
+        g_ms += ev[0].elapsed_time(ev[1])
+        s_ms += ev[1].elapsed_time(ev[2])
+    t = (g_ms + s_ms) / steps / 1000.0
+    return {"value": n / t, "unit": "markers/s", "gather_ms": g_ms / steps, "scatter_ms": s_ms / steps,
+            "marker_order": "random", "kernels": "reference gather_quadratic_3d + scatter_quadratic_3d, sm_100a"}
+
+
+def cpu_baseline(sample: int, threads: int = 0) -> dict:
+    """The reference's CPU kernels (OpenMP restatement of the Pyccel versions) on a sample."""
+    from oracle import oracle as O
+
+    dev = "cpu"
+    pos, w = make_markers(sample, dev, torch.float64, seed=7)
+    field = make_field(dev, torch.float64).numpy()
+    pos, w = pos.numpy(), w.numpy()
+    density = np.zeros((GRID, GRID, GRID, 1))
+    nthreads = threads or os.cpu_count() or 1
+    O.cpu_gather("quadratic", 2, pos[:, :1000], field, geometry(), nthreads)  # warm
+    t0 = time.perf_counter()
+    O.cpu_gather("quadratic", 2, pos, field, geometry(), nthreads)
+    t1 = time.perf_counter()
+    used = O.cpu_scatter("quadratic", 2, pos, w, density, geometry(), nthreads)
+    t2 = time.perf_counter()
+    seconds = t2 - t0
+    return {"value": sample / seconds, "unit": "markers/s", "cores": nthreads, "kind": "port",
+            "sample": f"{sample} markers of the workload (gather {t1 - t0:.3f} s on {nthreads} threads, "
+                      f"scatter {t2 - t1:.3f} s on {used} thread(s): the reference's 256^3 deposit "
+                      "runs serially, its per-thread grids exceed 16,777,216 values)"}
+
+
+def run_ours(args, world, rank, local) -> None:
+    device = torch.device("cuda", local)
+    dtype = torch.float64 if args.dtype == "f64" else torch.float32
+    itemsize = 8 if dtype == torch.float64 else 4
+    n = args.markers
+    step = Step(n, device, dtype)
+    pos, w = make_markers(n, device, dtype, seed=1 + rank)
+    from mpifield_b200 import _lib
+
+    # the headline: the full step on markers in random order
+    launches0 = _lib.library().mpf_launch_count()
+    with ClockSampler(local) as clocks:
+        seconds = time_loop(lambda: step.full(pos, w), args.steps, args.warmup, world, device)
+    launches = (_lib.library().mpf_launch_count() - launches0) // (args.steps + args.warmup) * args.steps
+    per_step = seconds / args.steps
+
+    # per-kernel times inside the full step (events on the launching stream)
+    sort_ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    g_ms = s_ms = sort_ms = 0.0
+    for _ in range(args.steps):
+        sort_ev[0].record()
+        t, ps, ws = step.sort(pos, w)
+        sort_ev[1].record()
+        step.gather_scatter(ps, ws, ev)
+        step.mf.unpermute(step.E, t.order, out=step.E_out)
+        torch.cuda.synchronize()
+        sort_ms += sort_ev[0].elapsed_time(sort_ev[1])
+        g_ms += ev[0].elapsed_time(ev[1])
+        s_ms += ev[1].elapsed_time(ev[2])
+    g_ms, s_ms, sort_ms = g_ms / args.steps, s_ms / args.steps, sort_ms / args.steps
+
+    # steady state: markers already in tile order
+    _, ps, ws = step.sort(pos, w)
+    steady = time_loop(lambda: step.gather_scatter(ps, ws), args.steps, args.warmup, world, device)
+
+    alg = algorithmic_bytes(n, itemsize)
+    peak, peak_kind = read_peak()
+    dominant = "gather" if g_ms >= s_ms else "scatter"
+    dom_ms = g_ms if dominant == "gather" else s_ms
+    achieved = alg[dominant] / (dom_ms / 1000.0) / 1e9
+    traffic = read_traffic(f"{dominant}_quadratic_3d_{args.dtype}")
+
+    e2e = None
+    if not args.no_e2e:
+        hp = torch.empty((3, n), dtype=dtype, pin_memory=True)
+        hw = torch.empty((1, n), dtype=dtype, pin_memory=True)
+        hp.copy_(pos)
+        hw.copy_(w)
+        hE = torch.empty((3, n), dtype=dtype, pin_memory=True)
+        hD = torch.empty(step.density.shape, dtype=dtype, pin_memory=True)
+        dpos, dw = torch.empty_like(pos), torch.empty_like(w)
+
+        def e2e_step():
+            dpos.copy_(hp, non_blocking=True)
+            dw.copy_(hw, non_blocking=True)
+            step.full(dpos, dw)
+            hE.copy_(step.E_out, non_blocking=True)
+            hD.copy_(step.density, non_blocking=True)
+
+        e2e_s = time_loop(e2e_step, max(2, args.steps // 2), 1, world, device)
+        e2e_steps = max(2, args.steps // 2)
+        e2e = {"value": n * world / (e2e_s / e2e_steps), "unit": "markers/s",
+               "h2d_bytes_per_step": (hp.numel() + hw.numel()) * itemsize,
+               "d2h_bytes_per_step": (hE.numel() + hD.numel()) * itemsize}
+
+    ref_cuda = None
+    if not args.no_ref_cuda and rank == 0 and dtype == torch.float64:
+        ref_cuda = ref_cuda_time(pos, w, step.field, step.density, step.E, max(2, args.steps // 2))
+
+    cpu = None
+    if not args.no_cpu and rank == 0 and world == 1:
+        cpu = cpu_baseline(1 << 21)
+
+    clock = clocks.summary()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": n * world / per_step, "unit": "markers/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_step * 1000.0,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": args.dtype, "data": "synthetic",
+            "config": {"workload": f"3D QUADRATIC gather E (3 comp) + scatter weights (1 comp), "
+                                   f"{GRID}^3 periodic, N={n} markers (80% uniform, 20% beam sigma 0.05), "
+                                   "random marker order; step = tile sort + permute + gather + scatter + "
+                                   "unpermute", "markers": n, "grid": [GRID] * 3, "tile": list(TILE),
+                       "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (positions 1.6 GB)"},
+            "steady_state": {"value": n * world / (steady / args.steps), "unit": "markers/s",
+                             "ms_per_step": steady / args.steps * 1000.0,
+                             "what": "gather + scatter on markers already in tile order"},
+            "kernel_ms": {"sort_and_permute": sort_ms, "gather": g_ms, "scatter": s_ms},
+            "roofline": {"bound": "hbm", "kernel": f"{dominant}_quadratic_3d", "achieved": achieved,
+                         "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                         "algorithmic_bytes": alg[dominant], "traffic": traffic},
+            "cpu_baseline": cpu, "ref_cuda": ref_cuda, "e2e": e2e, "gpu_launches": int(launches),
+            "clocks": clock,
+        }
+        print(json.dumps(line), flush=True)
+
+
+def run_reference(args, world, rank) -> None:
+    if rank != 0:
+        return
+    sample = 1 << 21
+    from oracle import oracle as O
+
+    pos, w = make_markers(sample, "cpu", torch.float64, seed=7)
+    pos, w = pos.numpy(), w.numpy()
+    field = make_field("cpu", torch.float64).numpy()
+    density = np.zeros((GRID, GRID, GRID, 1))
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        O.cpu_gather("quadratic", 2, pos[:, :65536], field, geometry(), threads)
+        O.cpu_scatter("quadratic", 2, pos[:, :65536], w[:, :65536], density, geometry(), threads)
+    t0 = time.perf_counter()
+    used = 1
+    for _ in range(args.steps):
+        O.cpu_gather("quadratic", 2, pos, field, geometry(), threads)
+        density[...] = 0.0
+        used = O.cpu_scatter("quadratic", 2, pos, w, density, geometry(), threads)
+    seconds = (time.perf_counter() - t0) / args.steps
+    value = sample / seconds
+    sample_text = (f"{sample} markers of the workload per step; gather on {threads} threads, scatter on "
+                   f"{used} thread(s) (the reference's rule for a 256^3 deposit)")
+    print(json.dumps({
+        "metric": METRIC, "value": value, "unit": "markers/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": seconds * 1000.0, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+        "config": {"workload": f"3D QUADRATIC gather E (3 comp) + scatter weights (1 comp), {GRID}^3 periodic, "
+                               "markers 80% uniform 20% beam; the reference's CPU kernels (OpenMP restatement "
+                               "of its Pyccel versions)", "markers": sample, "grid": [GRID] * 3},
+        "cpu_baseline": {"value": value, "unit": "markers/s", "cores": threads, "kind": "port",
+                         "sample": sample_text},
+        "e2e": {"value": value, "unit": "markers/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main() -> None:
+    args = parse()
+    world, rank, local = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,222 @@
+/*
+ * mpifield_b200.h -- the C ABI of the B200 particle-grid backend (libmpifield_b200.so).
+ *
+ * One entry point per operation of mpifield's kernel convention (src/mpifield/weighting.py:
+ * 22-38, src/mpifield/edges.py:23-31), with plain pointers and sizes. Every array lives
+ * in device memory of the current CUDA device; every call is asynchronous on `stream`
+ * (a cudaStream_t, NULL for the legacy default stream) and returns a status code
+ * (MPF_OK or one of the MPF_ERR_* below); no call traps, synchronises or allocates.
+ *
+ * Conventions shared by the calls:
+ *   - `ndim` is 1, 2 or 3. The grid is mpifield's BlockGrid.geometry
+ *     (src/mpifield/_types.py:27-44) split into four arrays of `ndim` entries:
+ *     `lower` (node 0), `cell` (node spacing), `num` (node count) and `code`
+ *     (0 bounded, 1 periodic, 2 clamped knots). On a clamped axis an array of degree p
+ *     holds num + p - 1 entries along it.
+ *   - Marker arrays are row-major rows of `n` elements, `stride` elements apart (the
+ *     (ndim, N) positions and (ncomp, N) values of the reference, which may have gaps
+ *     between rows). A stride of 0 means n.
+ *   - Grid arrays (fields, edge fields) are C-contiguous, components innermost:
+ *     extent + (ncomp,).
+ *   - `dtype` is MPF_F64 (double) or MPF_F32 (float); all the floating-point arrays of
+ *     a call have that type.
+ *   - `kind` picks the stencil arithmetic of the reference's weightings: MPF_LINEAR
+ *     (linear_cell.cuh, degree 1, LINEAR), MPF_QUADRATIC (quadratic_cell.cuh, degree 2,
+ *     QUADRATIC) or MPF_SPLINE (spline_cell.cuh, degree 0-3; CUBIC is degree 3).
+ *   - `tuning` may be NULL (the autotuned defaults).
+ */
+#ifndef MPIFIELD_B200_H
+#define MPIFIELD_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Exported from the shared library, whatever the default visibility of the build. */
+#if defined(__GNUC__)
+#define MPF_API __attribute__((visibility("default")))
+#else
+#define MPF_API
+#endif
+
+/* Status codes. */
+#define MPF_OK 0
+#define MPF_ERR_ARGUMENT 1     /* a dimension, kind, degree, code or count out of range */
+#define MPF_ERR_SHAPE 2        /* a stride or extent inconsistent with the sizes */
+#define MPF_ERR_ALIGNMENT 3    /* a pointer not aligned to its element type */
+#define MPF_ERR_WORKSPACE 4    /* a workspace smaller than the call needs */
+#define MPF_ERR_CUDA 5         /* a CUDA launch or attribute call failed */
+#define MPF_ERR_UNSUPPORTED 6  /* a combination this build does not provide */
+#define MPF_ERR_TIMEOUT 7      /* a bounded wait gave up (serving queue) */
+
+/* Stencil kinds. */
+#define MPF_LINEAR 0
+#define MPF_QUADRATIC 1
+#define MPF_SPLINE 2
+
+/* Element types. */
+#define MPF_F64 0
+#define MPF_F32 1
+
+/* Paths (mpf_tuning.path). */
+#define MPF_PATH_AUTO 0
+#define MPF_PATH_DIRECT 1 /* global memory only, one marker per thread */
+#define MPF_PATH_STAGED 2 /* shared-memory boxes per chunk of markers, else global */
+
+typedef struct mpf_tuning {
+    int32_t path;        /* MPF_PATH_* */
+    int32_t block;       /* threads per CTA (multiple of 32, <= 256); 0: default */
+    int32_t smem_bytes;  /* dynamic shared memory per CTA for a box; 0: default */
+    int32_t ctas_per_sm; /* resident CTAs per SM the grid is sized for; 0: default */
+} mpf_tuning;
+
+/* The library version, e.g. 10000 for 1.0.0. */
+MPF_API int mpf_version(void);
+
+/* The number of kernels this library has launched in the process (a diagnostic). */
+MPF_API int64_t mpf_launch_count(void);
+
+/* A static, human-readable name of a status code. */
+MPF_API const char* mpf_status_string(int status);
+
+/*
+ * Node gather: result(c, i) = sum_k W_k(x_i) field(k, c), overwriting result.
+ * Replaces the `gather(positions, field, result, *geometry)` kernels of mpifield's
+ * weightings: gather_{linear,quadratic,spline}_{1,2,3}d (src/mpifield/weighting.py:
+ * 233-250; e.g. src/mpifield/kernels/gather_spline_3d/gather_spline_3d_cuda.cu:11-53).
+ * positions (ndim, n), field extent + (ncomp,), result (ncomp, n).
+ */
+MPF_API int mpf_gather(int kind, int degree, int ndim, const void* positions, int64_t pos_stride,
+               int64_t n, const void* field, int64_t ncomp, void* result, int64_t res_stride,
+               const double* lower, const double* cell, const int32_t* num, const int32_t* code,
+               int dtype, const mpf_tuning* tuning, void* stream);
+
+/*
+ * Node scatter (deposit): field(k, c) += sum_i W_k(x_i) values(c, i). A marker whose
+ * values are all zero deposits nothing and its position is not read.
+ * Replaces `scatter(positions, values, field, *geometry)`: scatter_{linear,quadratic,
+ * spline}_{1,2,3}d (src/mpifield/weighting.py:195-213; e.g.
+ * src/mpifield/kernels/scatter_quadratic_3d/scatter_quadratic_3d_cuda.cu:12-60).
+ */
+MPF_API int mpf_scatter(int kind, int degree, int ndim, const void* positions, int64_t pos_stride,
+                const void* values, int64_t val_stride, int64_t n, void* field, int64_t ncomp,
+                const double* lower, const double* cell, const int32_t* num, const int32_t* code,
+                int dtype, const mpf_tuning* tuning, void* stream);
+
+/*
+ * Position gradient of a gather contracted with a cotangent, for reverse mode:
+ * grad(d, i) = sum_c cot(c, i) d/dx_d sum_k W_k(x_i) field(k, c), overwriting grad
+ * (ndim, n). The weight derivatives follow B_p' = B_{p-1}(.+1/2) - B_{p-1}(.-1/2)
+ * (src/mpifield/splines.py:9,77); zero where a bounded axis clamps the position. No
+ * kernel of the reference computes it.
+ */
+MPF_API int mpf_gather_grad(int kind, int degree, int ndim, const void* positions, int64_t pos_stride,
+                    int64_t n, const void* field, int64_t ncomp, const void* cotangent,
+                    int64_t cot_stride, void* grad, int64_t grad_stride, const double* lower,
+                    const double* cell, const int32_t* num, const int32_t* code, int dtype,
+                    void* stream);
+
+/*
+ * Path deposit: edges += the current of `charges` (n,) moving from start to end
+ * (ndim, n), edges extent + (ndim,). kind MPF_LINEAR with degree 1 is WHITNEY
+ * (deposit_paths_{1,2,3}d, src/mpifield/kernels/deposit_paths_3d/deposit_paths_3d_cuda.cu:
+ * 13-86); kind MPF_SPLINE with degree 1-3 is the spline-edge deposit of
+ * QUADRATIC_EDGES / CUBIC_EDGES (deposit_paths_spline_{1,2,3}d,
+ * deposit_paths_spline_3d_cuda.cu:14-130), replacing `deposit_paths(start, end, charges,
+ * edges, *geometry)` (src/mpifield/edges.py:187-215). A path with zero charge or a
+ * non-finite end deposits nothing.
+ */
+MPF_API int mpf_deposit_paths(int kind, int degree, int ndim, const void* start, int64_t start_stride,
+                      const void* end, int64_t end_stride, const void* charges, int64_t n,
+                      void* edges, const double* lower, const double* cell, const int32_t* num,
+                      const int32_t* code, int dtype, const mpf_tuning* tuning, void* stream);
+
+/*
+ * Edge gather: result(a, i) = sum W_{k,a}(x_i) edges(k, a) / cell[a], overwriting
+ * result (ndim, n). kind MPF_LINEAR (degree 1) is WHITNEY's gather_edges_{1,2,3}d,
+ * MPF_SPLINE with degree 1-3 gather_edges_spline_{1,2,3}d (src/mpifield/edges.py:
+ * 169-185).
+ */
+MPF_API int mpf_gather_edges(int kind, int degree, int ndim, const void* positions, int64_t pos_stride,
+                     int64_t n, const void* edges, void* result, int64_t res_stride,
+                     const double* lower, const double* cell, const int32_t* num,
+                     const int32_t* code, int dtype, void* stream);
+
+/*
+ * Halo fill of one block: on every periodic axis the `halo` low halo layers take the
+ * last `halo` owned layers and the high halo layers the first ones, axis by axis over
+ * the whole stored extent (corners included); other axes are left alone. `stored` is
+ * the extent with halos (owned + 2 halo per axis). Replaces Field.fill_halos on one
+ * process (src/mpifield/field.py:601-613, mpiarray's update_halos).
+ */
+MPF_API int mpf_halo_fill(void* field, int ndim, const int32_t* stored, int64_t ncomp, int32_t halo,
+                  const int32_t* periodic, int dtype, void* stream);
+
+/*
+ * Halo fold-back of one block after a deposit: on a periodic axis the high halo layers
+ * are added onto the first owned layers and the low ones onto the last, then every
+ * halo layer is zeroed (at a wall its values are dropped), axis by axis. Replaces
+ * Field.exchange_halos on one process (src/mpifield/field.py:615-630, mpiarray's
+ * accumulate_halos).
+ */
+MPF_API int mpf_halo_fold(void* field, int ndim, const int32_t* stored, int64_t ncomp, int32_t halo,
+                  const int32_t* periodic, int dtype, void* stream);
+
+/*
+ * dst += deposit / node volume over a block of `num` owned nodes stored with `halo`
+ * halo layers per axis (both arrays with the same storage), the volume being
+ * prod(cell), halved on the first and last node of a bounded axis. Halo nodes of dst
+ * are left unchanged. The last step of Field.deposit_density (src/mpifield/field.py:
+ * 1182-1218, node_volumes :563-588).
+ */
+MPF_API int mpf_add_density(void* dst, const void* deposit, int ndim, const int32_t* num, int32_t halo,
+                    int64_t ncomp, const double* cell, const int32_t* periodic, int dtype,
+                    void* stream);
+
+/*
+ * Cell-tile sort. keys[i] is the tile of marker i: the anchor node of its stencil per
+ * axis (LINEAR's left node, QUADRATIC's nearest node, the middle node of a spline
+ * stencil, the cell on a clamped axis) divided by tile[d], row-major over the
+ * ceil(extent / tile) tiles. With `values` non-NULL ((ncomp, n) rows) a marker whose
+ * values are all zero gets the key `num_tiles` without its position being read.
+ * order[j] is the marker of rank j in the stable ascending order of the keys (equal to
+ * numpy.argsort(keys, kind="stable")); tile_start (num_tiles + 2 entries) the first rank
+ * of every key and the count n at the end. `workspace` holds `mpf_sort_workspace_bytes`
+ * bytes of device memory. No reference kernel sorts (picnic's sort_by_cell is external,
+ * src/mpifield/kernels/scatter_linear_3d/scatter_linear_3d_pyccel.py:11-12).
+ */
+MPF_API int mpf_sort_workspace_bytes(int64_t n, int64_t num_tiles, size_t* bytes);
+MPF_API int mpf_sort_by_tile(int kind, int degree, int ndim, const void* positions, int64_t pos_stride,
+                     const void* values, int64_t val_stride, int64_t ncomp, int64_t n,
+                     const double* lower, const double* cell, const int32_t* num,
+                     const int32_t* code, const int32_t* tile, uint32_t* keys, int32_t* order,
+                     int64_t* tile_start, void* workspace, size_t workspace_bytes, int dtype,
+                     void* stream);
+
+/* The number of tiles of a grid for mpf_sort_by_tile, into *num_tiles. */
+MPF_API int mpf_num_tiles(int kind, int degree, int ndim, const int32_t* num, const int32_t* code,
+                  const int32_t* tile, int64_t* num_tiles);
+
+/*
+ * dst(r, j) = src(r, order[j]) for r < rows, j < n: a marker array permuted into sorted
+ * order (rows of n elements, strides in elements). dst and src must not overlap. An
+ * order entry outside [0, n) reads nothing and gives NaN.
+ */
+MPF_API int mpf_permute_rows(void* dst, int64_t dst_stride, const void* src, int64_t src_stride,
+                     int64_t rows, const int32_t* order, int64_t n, int dtype, void* stream);
+
+/*
+ * dst(r, order[j]) = src(r, j): the inverse of mpf_permute_rows, returning results computed
+ * in sorted order to the markers' own order. An order entry outside [0, n) writes nothing.
+ */
+MPF_API int mpf_unpermute_rows(void* dst, int64_t dst_stride, const void* src, int64_t src_stride,
+                               int64_t rows, const int32_t* order, int64_t n, int dtype, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MPIFIELD_B200_H */

@@ -1,0 +1,420 @@
+// mpf_capi.cu -- the extern "C" entry points of include/mpifield_b200.h: argument checks
+// (the ValueErrors the reference raises in Python before a kernel, src/mpifield/
+// weighting.py:91-97,156-164 and edges.py:145-167,210-213, become status codes here) and
+// the dispatch to the typed launchers.
+#include <atomic>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+
+#include "mpf_internal.h"
+#include "mpf_stencil.cuh"
+#include "mpifield_b200.h"
+
+namespace mpf {
+
+static std::atomic<long long> g_launches{0};
+
+void count_launches(int k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
+
+int sm_count() {
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess) return 148;
+    static int cached[64] = {0};
+    if (device < 0 || device >= 64) return 148;
+    if (cached[device] == 0) {
+        int count = 0;
+        if (cudaDeviceGetAttribute(&count, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || count <= 0)
+            count = 148;
+        cached[device] = count;
+    }
+    return cached[device];
+}
+
+static bool valid_kind(int kind, int degree) {
+    if (kind == MPF_LINEAR) return degree == 1;
+    if (kind == MPF_QUADRATIC) return degree == 2;
+    if (kind == MPF_SPLINE) return degree >= 0 && degree <= 3;
+    return false;
+}
+
+// The checks of a grid: dimensions, positive finite spacing, node counts (two at least
+// on bounded and clamped axes, whose stencils take the last cell), codes, and clamped
+// axes only for spline stencils of degree >= 1 (src/mpifield/weighting.py:91-97).
+static int check_grid(int kind, int degree, int ndim, const double* lower, const double* cell,
+                      const int32_t* num, const int32_t* code) {
+    if (ndim < 1 || ndim > 3) return MPF_ERR_ARGUMENT;
+    if (!lower || !cell || !num || !code) return MPF_ERR_ARGUMENT;
+    for (int d = 0; d < ndim; ++d) {
+        if (!std::isfinite(lower[d]) || !std::isfinite(cell[d]) || cell[d] == 0.0) return MPF_ERR_ARGUMENT;
+        if (code[d] < 0 || code[d] > 2) return MPF_ERR_ARGUMENT;
+        if (num[d] < 1 || num[d] > (1 << 28)) return MPF_ERR_ARGUMENT;
+        if (code[d] != PERIODIC && num[d] < 2) return MPF_ERR_ARGUMENT;
+        if (code[d] == CLAMPED && (kind != MPF_SPLINE || degree < 1)) return MPF_ERR_UNSUPPORTED;
+    }
+    return MPF_OK;
+}
+
+template <typename T>
+static Grid<T> make_grid(int ndim, int degree, const double* lower, const double* cell, const int32_t* num,
+                         const int32_t* code) {
+    Grid<T> g;
+    for (int d = 0; d < 3; ++d) {
+        const bool on = d < ndim;
+        g.lower[d] = on ? (T)lower[d] : T(0);
+        g.cell[d] = on ? (T)cell[d] : T(1);
+        g.num[d] = on ? num[d] : 1;
+        g.code[d] = on ? code[d] : PERIODIC;
+        g.ext[d] = on ? axis_extent(num[d], code[d], degree) : 1;
+    }
+    return g;
+}
+
+static bool aligned(const void* p, int dtype) {
+    const uintptr_t size = dtype == MPF_F64 ? 8 : 4;
+    return (reinterpret_cast<uintptr_t>(p) % size) == 0;
+}
+
+static int check_rows(const void* p, int64_t& stride, int64_t n, int rows, int dtype) {
+    if (stride == 0) stride = n;
+    if (stride < n || stride < 0) return MPF_ERR_SHAPE;
+    if (n > 0 && rows > 0) {
+        if (!p) return MPF_ERR_ARGUMENT;
+        if (!aligned(p, dtype)) return MPF_ERR_ALIGNMENT;
+    }
+    return MPF_OK;
+}
+
+static Tuning tuning_of(const mpf_tuning* t) {
+    Tuning u{0, 0, 0, 0};
+    if (t) {
+        u.path = t->path;
+        u.block = t->block;
+        u.smem_bytes = t->smem_bytes;
+        u.ctas_per_sm = t->ctas_per_sm;
+    }
+    return u;
+}
+
+template <typename T>
+static NodeArgs<T> node_args(int ndim, int degree, const double* lower, const double* cell, const int32_t* num,
+                             const int32_t* code) {
+    NodeArgs<T> a;
+    std::memset(&a, 0, sizeof(a));
+    a.g = make_grid<T>(ndim, degree, lower, cell, num, code);
+    return a;
+}
+
+}  // namespace mpf
+
+using namespace mpf;
+
+#define MPF_TRY(expr)                     \
+    do {                                  \
+        const int status_ = (expr);       \
+        if (status_ != MPF_OK) return status_; \
+    } while (0)
+
+extern "C" {
+
+int mpf_version(void) { return 10000; }
+
+int64_t mpf_launch_count(void) { return (int64_t)g_launches.load(std::memory_order_relaxed); }
+
+const char* mpf_status_string(int status) {
+    switch (status) {
+        case MPF_OK: return "ok";
+        case MPF_ERR_ARGUMENT: return "invalid argument";
+        case MPF_ERR_SHAPE: return "inconsistent shape or stride";
+        case MPF_ERR_ALIGNMENT: return "misaligned pointer";
+        case MPF_ERR_WORKSPACE: return "workspace too small";
+        case MPF_ERR_CUDA: return "CUDA error";
+        case MPF_ERR_UNSUPPORTED: return "unsupported combination";
+        case MPF_ERR_TIMEOUT: return "timed out";
+    }
+    return "unknown status";
+}
+
+int mpf_gather(int kind, int degree, int ndim, const void* positions, int64_t pos_stride, int64_t n,
+               const void* field, int64_t ncomp, void* result, int64_t res_stride, const double* lower,
+               const double* cell, const int32_t* num, const int32_t* code, int dtype,
+               const mpf_tuning* tuning, void* stream) {
+    if (!valid_kind(kind, degree) || (dtype != MPF_F64 && dtype != MPF_F32)) return MPF_ERR_ARGUMENT;
+    MPF_TRY(check_grid(kind, degree, ndim, lower, cell, num, code));
+    if (n < 0 || ncomp < 1 || ncomp > (1 << 20)) return MPF_ERR_ARGUMENT;
+    MPF_TRY(check_rows(positions, pos_stride, n, ndim, dtype));
+    MPF_TRY(check_rows(result, res_stride, n, (int)ncomp, dtype));
+    if (n == 0) return MPF_OK;
+    if (!field) return MPF_ERR_ARGUMENT;
+    if (!aligned(field, dtype)) return MPF_ERR_ALIGNMENT;
+    const Tuning t = tuning_of(tuning);
+    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (dtype == MPF_F64) {
+        NodeArgs<double> a = node_args<double>(ndim, degree, lower, cell, num, code);
+        a.pos = (const double*)positions; a.pos_stride = pos_stride;
+        a.field_in = (const double*)field; a.result = (double*)result; a.res_stride = res_stride;
+        a.n = n; a.ncomp = (int)ncomp;
+        return launch_gather<double>(kind, degree, ndim, a, t, s);
+    }
+    NodeArgs<float> a = node_args<float>(ndim, degree, lower, cell, num, code);
+    a.pos = (const float*)positions; a.pos_stride = pos_stride;
+    a.field_in = (const float*)field; a.result = (float*)result; a.res_stride = res_stride;
+    a.n = n; a.ncomp = (int)ncomp;
+    return launch_gather<float>(kind, degree, ndim, a, t, s);
+}
+
+int mpf_scatter(int kind, int degree, int ndim, const void* positions, int64_t pos_stride, const void* values,
+                int64_t val_stride, int64_t n, void* field, int64_t ncomp, const double* lower,
+                const double* cell, const int32_t* num, const int32_t* code, int dtype,
+                const mpf_tuning* tuning, void* stream) {
+    if (!valid_kind(kind, degree) || (dtype != MPF_F64 && dtype != MPF_F32)) return MPF_ERR_ARGUMENT;
+    MPF_TRY(check_grid(kind, degree, ndim, lower, cell, num, code));
+    if (n < 0 || ncomp < 1 || ncomp > (1 << 20)) return MPF_ERR_ARGUMENT;
+    MPF_TRY(check_rows(positions, pos_stride, n, ndim, dtype));
+    MPF_TRY(check_rows(values, val_stride, n, (int)ncomp, dtype));
+    if (n == 0) return MPF_OK;
+    if (!field) return MPF_ERR_ARGUMENT;
+    if (!aligned(field, dtype)) return MPF_ERR_ALIGNMENT;
+    const Tuning t = tuning_of(tuning);
+    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (dtype == MPF_F64) {
+        NodeArgs<double> a = node_args<double>(ndim, degree, lower, cell, num, code);
+        a.pos = (const double*)positions; a.pos_stride = pos_stride;
+        a.values = (const double*)values; a.val_stride = val_stride;
+        a.field_out = (double*)field; a.n = n; a.ncomp = (int)ncomp;
+        return launch_scatter<double>(kind, degree, ndim, a, t, s);
+    }
+    NodeArgs<float> a = node_args<float>(ndim, degree, lower, cell, num, code);
+    a.pos = (const float*)positions; a.pos_stride = pos_stride;
+    a.values = (const float*)values; a.val_stride = val_stride;
+    a.field_out = (float*)field; a.n = n; a.ncomp = (int)ncomp;
+    return launch_scatter<float>(kind, degree, ndim, a, t, s);
+}
+
+int mpf_gather_grad(int kind, int degree, int ndim, const void* positions, int64_t pos_stride, int64_t n,
+                    const void* field, int64_t ncomp, const void* cotangent, int64_t cot_stride, void* grad,
+                    int64_t grad_stride, const double* lower, const double* cell, const int32_t* num,
+                    const int32_t* code, int dtype, void* stream) {
+    if (!valid_kind(kind, degree) || (dtype != MPF_F64 && dtype != MPF_F32)) return MPF_ERR_ARGUMENT;
+    MPF_TRY(check_grid(kind, degree, ndim, lower, cell, num, code));
+    if (n < 0 || ncomp < 1 || ncomp > (1 << 20)) return MPF_ERR_ARGUMENT;
+    MPF_TRY(check_rows(positions, pos_stride, n, ndim, dtype));
+    MPF_TRY(check_rows(cotangent, cot_stride, n, (int)ncomp, dtype));
+    MPF_TRY(check_rows(grad, grad_stride, n, ndim, dtype));
+    if (n == 0) return MPF_OK;
+    if (!field) return MPF_ERR_ARGUMENT;
+    if (!aligned(field, dtype)) return MPF_ERR_ALIGNMENT;
+    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (dtype == MPF_F64) {
+        NodeArgs<double> a = node_args<double>(ndim, degree, lower, cell, num, code);
+        a.pos = (const double*)positions; a.pos_stride = pos_stride;
+        a.field_in = (const double*)field; a.values = (const double*)cotangent; a.val_stride = cot_stride;
+        a.result = (double*)grad; a.res_stride = grad_stride; a.n = n; a.ncomp = (int)ncomp;
+        return launch_gather_grad<double>(kind, degree, ndim, a, s);
+    }
+    NodeArgs<float> a = node_args<float>(ndim, degree, lower, cell, num, code);
+    a.pos = (const float*)positions; a.pos_stride = pos_stride;
+    a.field_in = (const float*)field; a.values = (const float*)cotangent; a.val_stride = cot_stride;
+    a.result = (float*)grad; a.res_stride = grad_stride; a.n = n; a.ncomp = (int)ncomp;
+    return launch_gather_grad<float>(kind, degree, ndim, a, s);
+}
+
+static bool valid_edge_kind(int kind, int degree) {
+    if (kind == MPF_LINEAR) return degree == 1;
+    if (kind == MPF_SPLINE) return degree >= 1 && degree <= 3;
+    return false;
+}
+
+int mpf_deposit_paths(int kind, int degree, int ndim, const void* start, int64_t start_stride, const void* end,
+                      int64_t end_stride, const void* charges, int64_t n, void* edges, const double* lower,
+                      const double* cell, const int32_t* num, const int32_t* code, int dtype,
+                      const mpf_tuning* tuning, void* stream) {
+    (void)tuning;
+    if (!valid_edge_kind(kind, degree) || (dtype != MPF_F64 && dtype != MPF_F32)) return MPF_ERR_ARGUMENT;
+    MPF_TRY(check_grid(kind == MPF_LINEAR ? MPF_LINEAR : MPF_SPLINE, degree, ndim, lower, cell, num, code));
+    if (n < 0) return MPF_ERR_ARGUMENT;
+    MPF_TRY(check_rows(start, start_stride, n, ndim, dtype));
+    MPF_TRY(check_rows(end, end_stride, n, ndim, dtype));
+    int64_t one = n;
+    MPF_TRY(check_rows(charges, one, n, 1, dtype));
+    if (n == 0) return MPF_OK;
+    if (!edges) return MPF_ERR_ARGUMENT;
+    if (!aligned(edges, dtype)) return MPF_ERR_ALIGNMENT;
+    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (dtype == MPF_F64) {
+        PathArgs<double> a;
+        std::memset(&a, 0, sizeof(a));
+        a.g = make_grid<double>(ndim, degree, lower, cell, num, code);
+        a.start = (const double*)start; a.start_stride = start_stride;
+        a.end = (const double*)end; a.end_stride = end_stride;
+        a.charges = (const double*)charges; a.edges_out = (double*)edges; a.n = n;
+        return launch_deposit_paths<double>(kind, degree, ndim, a, s);
+    }
+    PathArgs<float> a;
+    std::memset(&a, 0, sizeof(a));
+    a.g = make_grid<float>(ndim, degree, lower, cell, num, code);
+    a.start = (const float*)start; a.start_stride = start_stride;
+    a.end = (const float*)end; a.end_stride = end_stride;
+    a.charges = (const float*)charges; a.edges_out = (float*)edges; a.n = n;
+    return launch_deposit_paths<float>(kind, degree, ndim, a, s);
+}
+
+int mpf_gather_edges(int kind, int degree, int ndim, const void* positions, int64_t pos_stride, int64_t n,
+                     const void* edges, void* result, int64_t res_stride, const double* lower,
+                     const double* cell, const int32_t* num, const int32_t* code, int dtype, void* stream) {
+    if (!valid_edge_kind(kind, degree) || (dtype != MPF_F64 && dtype != MPF_F32)) return MPF_ERR_ARGUMENT;
+    MPF_TRY(check_grid(kind == MPF_LINEAR ? MPF_LINEAR : MPF_SPLINE, degree, ndim, lower, cell, num, code));
+    if (n < 0) return MPF_ERR_ARGUMENT;
+    MPF_TRY(check_rows(positions, pos_stride, n, ndim, dtype));
+    MPF_TRY(check_rows(result, res_stride, n, ndim, dtype));
+    if (n == 0) return MPF_OK;
+    if (!edges) return MPF_ERR_ARGUMENT;
+    if (!aligned(edges, dtype)) return MPF_ERR_ALIGNMENT;
+    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (dtype == MPF_F64) {
+        PathArgs<double> a;
+        std::memset(&a, 0, sizeof(a));
+        a.g = make_grid<double>(ndim, degree, lower, cell, num, code);
+        a.pos = (const double*)positions; a.pos_stride = pos_stride;
+        a.edges_in = (const double*)edges; a.result = (double*)result; a.res_stride = res_stride; a.n = n;
+        return launch_gather_edges<double>(kind, degree, ndim, a, s);
+    }
+    PathArgs<float> a;
+    std::memset(&a, 0, sizeof(a));
+    a.g = make_grid<float>(ndim, degree, lower, cell, num, code);
+    a.pos = (const float*)positions; a.pos_stride = pos_stride;
+    a.edges_in = (const float*)edges; a.result = (float*)result; a.res_stride = res_stride; a.n = n;
+    return launch_gather_edges<float>(kind, degree, ndim, a, s);
+}
+
+static int check_block(void* field, int ndim, const int32_t* extent, int64_t ncomp, int32_t halo,
+                       const int32_t* periodic, int dtype, bool stored) {
+    if (ndim < 1 || ndim > 3 || !extent || !periodic || ncomp < 1 || halo < 0) return MPF_ERR_ARGUMENT;
+    if (dtype != MPF_F64 && dtype != MPF_F32) return MPF_ERR_ARGUMENT;
+    for (int d = 0; d < ndim; ++d) {
+        const int64_t owned = stored ? (int64_t)extent[d] - 2 * (int64_t)halo : extent[d];
+        if (owned < 1 || owned < halo) return MPF_ERR_SHAPE;
+    }
+    if (!field) return MPF_ERR_ARGUMENT;
+    if (!aligned(field, dtype)) return MPF_ERR_ALIGNMENT;
+    return MPF_OK;
+}
+
+int mpf_halo_fill(void* field, int ndim, const int32_t* stored, int64_t ncomp, int32_t halo,
+                  const int32_t* periodic, int dtype, void* stream) {
+    MPF_TRY(check_block(field, ndim, stored, ncomp, halo, periodic, dtype, true));
+    if (halo == 0) return MPF_OK;
+    return halo_fill(field, ndim, stored, ncomp, halo, periodic, dtype, static_cast<cudaStream_t>(stream));
+}
+
+int mpf_halo_fold(void* field, int ndim, const int32_t* stored, int64_t ncomp, int32_t halo,
+                  const int32_t* periodic, int dtype, void* stream) {
+    MPF_TRY(check_block(field, ndim, stored, ncomp, halo, periodic, dtype, true));
+    if (halo == 0) return MPF_OK;
+    return halo_fold(field, ndim, stored, ncomp, halo, periodic, dtype, static_cast<cudaStream_t>(stream));
+}
+
+int mpf_add_density(void* dst, const void* deposit, int ndim, const int32_t* num, int32_t halo, int64_t ncomp,
+                    const double* cell, const int32_t* periodic, int dtype, void* stream) {
+    MPF_TRY(check_block(dst, ndim, num, ncomp, halo, periodic, dtype, false));
+    if (!deposit || !cell) return MPF_ERR_ARGUMENT;
+    if (!aligned(deposit, dtype)) return MPF_ERR_ALIGNMENT;
+    for (int d = 0; d < ndim; ++d)
+        if (!std::isfinite(cell[d]) || cell[d] == 0.0) return MPF_ERR_ARGUMENT;
+    return add_density(dst, deposit, ndim, num, halo, ncomp, cell, periodic, dtype, static_cast<cudaStream_t>(stream));
+}
+
+int mpf_num_tiles(int kind, int degree, int ndim, const int32_t* num, const int32_t* code, const int32_t* tile,
+                  int64_t* num_tiles) {
+    if (!valid_kind(kind, degree) || ndim < 1 || ndim > 3 || !num || !code || !tile || !num_tiles)
+        return MPF_ERR_ARGUMENT;
+    int64_t total = 1;
+    for (int d = 0; d < ndim; ++d) {
+        if (tile[d] < 1 || num[d] < 1 || code[d] < 0 || code[d] > 2) return MPF_ERR_ARGUMENT;
+        const int64_t e = axis_extent(num[d], code[d], degree);
+        total *= (e + tile[d] - 1) / tile[d];
+        if (total >= (int64_t)1 << 31) return MPF_ERR_ARGUMENT;
+    }
+    *num_tiles = total;
+    return MPF_OK;
+}
+
+int mpf_sort_workspace_bytes(int64_t n, int64_t num_tiles, size_t* bytes) {
+    if (n < 0 || n > INT32_MAX || num_tiles < 1 || !bytes) return MPF_ERR_ARGUMENT;
+    *bytes = sort_workspace_bytes(n);
+    return MPF_OK;
+}
+
+int mpf_sort_by_tile(int kind, int degree, int ndim, const void* positions, int64_t pos_stride, const void* values,
+                     int64_t val_stride, int64_t ncomp, int64_t n, const double* lower, const double* cell,
+                     const int32_t* num, const int32_t* code, const int32_t* tile, uint32_t* keys, int32_t* order,
+                     int64_t* tile_start, void* workspace, size_t workspace_bytes, int dtype, void* stream) {
+    if (!valid_kind(kind, degree) || (dtype != MPF_F64 && dtype != MPF_F32)) return MPF_ERR_ARGUMENT;
+    MPF_TRY(check_grid(kind, degree, ndim, lower, cell, num, code));
+    if (n < 0 || n > INT32_MAX) return MPF_ERR_ARGUMENT;
+    int64_t ntiles = 0;
+    MPF_TRY(mpf_num_tiles(kind, degree, ndim, num, code, tile, &ntiles));
+    MPF_TRY(check_rows(positions, pos_stride, n, ndim, dtype));
+    if (values) {
+        if (ncomp < 1) return MPF_ERR_ARGUMENT;
+        MPF_TRY(check_rows(values, val_stride, n, (int)ncomp, dtype));
+    }
+    if (!keys || !order || !tile_start) return MPF_ERR_ARGUMENT;
+    if (workspace_bytes < sort_workspace_bytes(n) || (!workspace && n > 0)) return MPF_ERR_WORKSPACE;
+    if ((reinterpret_cast<uintptr_t>(workspace) % 256) != 0) return MPF_ERR_ALIGNMENT;
+    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (n > 0) {
+        int st;
+        if (dtype == MPF_F64) {
+            KeyArgs<double> a;
+            std::memset(&a, 0, sizeof(a));
+            a.g = make_grid<double>(ndim, degree, lower, cell, num, code);
+            a.pos = (const double*)positions; a.pos_stride = pos_stride;
+            a.values = (const double*)values; a.val_stride = val_stride; a.ncomp = ncomp; a.n = n;
+            for (int d = 0; d < 3; ++d) {
+                a.tile[d] = d < ndim ? tile[d] : 1;
+                a.ntiles[d] = d < ndim ? (a.g.ext[d] + a.tile[d] - 1) / a.tile[d] : 1;
+            }
+            a.sentinel = (uint32_t)ntiles; a.keys = keys;
+            st = tile_keys<double>(kind, degree, ndim, a, s);
+        } else {
+            KeyArgs<float> a;
+            std::memset(&a, 0, sizeof(a));
+            a.g = make_grid<float>(ndim, degree, lower, cell, num, code);
+            a.pos = (const float*)positions; a.pos_stride = pos_stride;
+            a.values = (const float*)values; a.val_stride = val_stride; a.ncomp = ncomp; a.n = n;
+            for (int d = 0; d < 3; ++d) {
+                a.tile[d] = d < ndim ? tile[d] : 1;
+                a.ntiles[d] = d < ndim ? (a.g.ext[d] + a.tile[d] - 1) / a.tile[d] : 1;
+            }
+            a.sentinel = (uint32_t)ntiles; a.keys = keys;
+            st = tile_keys<float>(kind, degree, ndim, a, s);
+        }
+        if (st != MPF_OK) return st;
+    }
+    return sort_keys(keys, n, ntiles, order, tile_start, workspace, s);
+}
+
+int mpf_permute_rows(void* dst, int64_t dst_stride, const void* src, int64_t src_stride, int64_t rows,
+                     const int32_t* order, int64_t n, int dtype, void* stream) {
+    if (dtype != MPF_F64 && dtype != MPF_F32) return MPF_ERR_ARGUMENT;
+    if (n < 0 || rows < 0) return MPF_ERR_ARGUMENT;
+    MPF_TRY(check_rows(dst, dst_stride, n, (int)rows, dtype));
+    MPF_TRY(check_rows(src, src_stride, n, (int)rows, dtype));
+    if (n == 0 || rows == 0) return MPF_OK;
+    if (!order) return MPF_ERR_ARGUMENT;
+    return permute_rows(dst, dst_stride, src, src_stride, rows, order, n, dtype, static_cast<cudaStream_t>(stream));
+}
+
+int mpf_unpermute_rows(void* dst, int64_t dst_stride, const void* src, int64_t src_stride, int64_t rows,
+                       const int32_t* order, int64_t n, int dtype, void* stream) {
+    if (dtype != MPF_F64 && dtype != MPF_F32) return MPF_ERR_ARGUMENT;
+    if (n < 0 || rows < 0) return MPF_ERR_ARGUMENT;
+    MPF_TRY(check_rows(dst, dst_stride, n, (int)rows, dtype));
+    MPF_TRY(check_rows(src, src_stride, n, (int)rows, dtype));
+    if (n == 0 || rows == 0) return MPF_OK;
+    if (!order) return MPF_ERR_ARGUMENT;
+    return unpermute_rows(dst, dst_stride, src, src_stride, rows, order, n, dtype, static_cast<cudaStream_t>(stream));
+}
+
+}  // extern "C"

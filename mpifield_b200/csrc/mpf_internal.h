@@ -1,0 +1,114 @@
+// mpf_internal.h -- argument blocks and launch entry points shared by the .cu files.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace mpf {
+
+// The grid of a block, as the kernels see it (src/mpifield/_types.py:27-44): the
+// position of node 0, the node spacing, the node count and the boundary code per axis,
+// and the array extent (num, or num + P - 1 on a clamped axis).
+template <typename T> struct Grid {
+    T lower[3];
+    T cell[3];
+    int num[3];
+    int code[3];
+    int ext[3];
+};
+
+// A node gather, scatter or position-gradient gather.
+template <typename T> struct NodeArgs {
+    Grid<T> g;
+    const T* pos;        // (ndim, n), rows pos_stride apart
+    int64_t pos_stride;
+    const T* values;     // scatter: (ncomp, n); gradient: the cotangent (ncomp, n)
+    int64_t val_stride;
+    const T* field_in;   // gather / gradient: ext + (ncomp,), C-contiguous
+    T* field_out;        // scatter
+    T* result;           // gather: (ncomp, n); gradient: (ndim, n)
+    int64_t res_stride;
+    int64_t n;
+    int ncomp;
+    int capacity;        // shared-memory box capacity, in elements of T
+    int force_global;    // 1: never stage (the direct path), for tests and unsorted input
+};
+
+// The tuning of one launch (the autotuned table supplies it; zero fields take defaults).
+struct Tuning {
+    int path;        // 0 auto, 1 direct (global memory only), 2 staged boxes
+    int block;       // threads per CTA
+    int smem_bytes;  // dynamic shared memory per CTA for the box
+    int ctas_per_sm; // resident CTAs per SM the grid is sized for
+};
+
+template <typename T>
+int launch_gather(int kind, int degree, int ndim, const NodeArgs<T>& a, const Tuning& t,
+                  cudaStream_t stream);
+template <typename T>
+int launch_scatter(int kind, int degree, int ndim, const NodeArgs<T>& a, const Tuning& t,
+                   cudaStream_t stream);
+template <typename T>
+int launch_gather_grad(int kind, int degree, int ndim, const NodeArgs<T>& a, cudaStream_t stream);
+
+// A path deposit or an edge gather.
+template <typename T> struct PathArgs {
+    Grid<T> g;
+    const T* start;
+    int64_t start_stride;
+    const T* end;
+    int64_t end_stride;
+    const T* charges;
+    const T* pos;  // edge gather
+    int64_t pos_stride;
+    const T* edges_in;
+    T* edges_out;
+    T* result;
+    int64_t res_stride;
+    int64_t n;
+};
+
+// The cell-tile keys of the markers.
+template <typename T> struct KeyArgs {
+    Grid<T> g;
+    const T* pos;
+    int64_t pos_stride;
+    const T* values;
+    int64_t val_stride;
+    int64_t ncomp;
+    int64_t n;
+    int tile[3];
+    int64_t ntiles[3];
+    uint32_t sentinel;
+    uint32_t* keys;
+};
+
+template <typename T>
+int launch_deposit_paths(int kind, int degree, int ndim, const PathArgs<T>& a, cudaStream_t stream);
+template <typename T>
+int launch_gather_edges(int kind, int degree, int ndim, const PathArgs<T>& a, cudaStream_t stream);
+
+int halo_fill(void* f, int ndim, const int32_t* stored, int64_t ncomp, int h, const int32_t* periodic,
+              int dtype, cudaStream_t stream);
+int halo_fold(void* f, int ndim, const int32_t* stored, int64_t ncomp, int h, const int32_t* periodic,
+              int dtype, cudaStream_t stream);
+int add_density(void* dst, const void* dep, int ndim, const int32_t* num, int h, int64_t ncomp,
+                const double* cell, const int32_t* periodic, int dtype, cudaStream_t stream);
+
+template <typename T>
+int tile_keys(int kind, int degree, int ndim, const KeyArgs<T>& a, cudaStream_t stream);
+size_t sort_workspace_bytes(int64_t n);
+int sort_keys(const uint32_t* keys, int64_t n, int64_t num_tiles, int32_t* order, int64_t* tile_start,
+              void* workspace, cudaStream_t stream);
+int permute_rows(void* dst, int64_t ds, const void* src, int64_t ss, int64_t rows, const int32_t* order,
+                 int64_t n, int dtype, cudaStream_t stream);
+
+int unpermute_rows(void* dst, int64_t ds, const void* src, int64_t ss, int64_t rows, const int32_t* order,
+                   int64_t n, int dtype, cudaStream_t stream);
+
+int sm_count();
+
+// Counts kernel launches of this library (read by mpf_launch_count).
+void count_launches(int k);
+
+}  // namespace mpf

@@ -1,0 +1,507 @@
+// mpf_paths.cuh -- the charge-conserving path deposits and the edge gathers.
+//
+// Edge fields are extent + (ndim,): entry (k, a) is the line integral along the edge from
+// node k to its neighbour along axis a (src/mpifield/edges.py:1-31).
+//
+// WHITNEY (degree 1) follows deposit_paths_{1,2,3}d of mpifield
+// (src/mpifield/kernels/deposit_paths_3d/deposit_paths_3d_cuda.cu:13-86 with
+// whitney_cell.cuh:12-53): a straight path in cells is cut where it crosses a grid plane
+// (the next plane of every axis, advanced together on ties), each piece clamped on
+// bounded axes; the piece adds q times its length along an axis to the cell's edges
+// along that axis, times their weights averaged over the piece (the midpoint's, plus or
+// minus delta_u delta_w / 12 in 3D).
+//
+// The spline-edge deposit of degree P = 1..3 follows deposit_paths_spline_{1,2,3}d
+// (deposit_paths_spline_3d_cuda.cu:14-130 with spline_edges.cuh:16-135): stretches of at
+// most 4 cells, each cut at its knot planes (half-integers for even P; the nodes on a
+// clamped axis) and at the walls of bounded axes, every clamped piece integrated with
+// (P - 1 + (ndim - 1) P) / 2 + 1 Gauss-Legendre points; at a point the edges along axis a
+// weigh B_{P-1}(r_a - k_a - 1/2) prod_{b != a} B_P(r_b - k_b), and edges past a bounded
+// wall do not exist. Where the reference gathers every cut of a stretch into a 32-entry
+// array and insertion-sorts it, this kernel merges the per-axis streams of crossing
+// times in registers: the same times, each computed by the same formula, taken in the
+// same ascending order, so the pieces are the same.
+#pragma once
+#include "mpf_internal.h"
+#include "mpf_stencil.cuh"
+
+namespace mpf {
+
+
+// The longest a path may be, in pieces per stretch walk (WHITNEY) or stretches (spline):
+// a bound on the work of one thread for absurd inputs; paths of physical length (a few
+// cells per step) never reach it.
+constexpr int kMaxPathSteps = 1 << 16;
+
+template <typename T> __device__ __forceinline__ T clamp_to_axis(T rel, int num, int code) {
+    if (code == PERIODIC) return rel;
+    if (rel < T(0)) return T(0);
+    if (rel > T(num) - T(1)) return T(num) - T(1);
+    return rel;
+}
+
+// Adds v to edge (node index per axis, axis) with a global atomic.
+template <typename T, int NDIM> struct GlobalEdgeSink {
+    T* edges;
+    int ext[3];
+    __device__ __forceinline__ void add(const int* node, int axis, T v) const {
+        int64_t k = node[0];
+#pragma unroll
+        for (int d = 1; d < NDIM; ++d) k = k * ext[d] + node[d];
+        atomicAdd(edges + k * NDIM + axis, v);
+    }
+};
+
+// The linear (Whitney) cell of a position: left and right nodes, the right weight.
+template <typename T>
+__device__ __forceinline__ void linear_nodes(T rel, int num, int code, int& left, int& right, T& f) {
+    T w[2];
+    const int base = axis_stencil<T, LINEAR, 1>(rel, num, code, w);
+    left = map_node(base, num, code);
+    right = map_node(base + 1, num, code);
+    f = w[1];
+}
+
+template <typename T, int NDIM, typename Sink>
+__device__ void whitney_path(T q, const T* a, const T* b, const Grid<T>& g, const Sink& sink) {
+    T dl[NDIM], plane[NDIM], step[NDIM], p0[NDIM];
+#pragma unroll
+    for (int d = 0; d < NDIM; ++d) {
+        dl[d] = b[d] - a[d];
+        if (dl[d] < T(0)) {
+            plane[d] = ceil(a[d]) - T(1);
+            step[d] = T(-1);
+        } else {
+            plane[d] = floor(a[d]) + T(1);
+            step[d] = T(1);
+        }
+        p0[d] = clamp_to_axis(a[d], g.num[d], g.code[d]);
+    }
+    T time = T(0);
+    for (int guard = 0; time < T(1) && guard < kMaxPathSteps; ++guard) {
+        T times[NDIM];
+        T following = T(1);
+#pragma unroll
+        for (int d = 0; d < NDIM; ++d) {
+            times[d] = dl[d] != T(0) ? (plane[d] - a[d]) / dl[d] : T(2);
+            if (times[d] < following) following = times[d];
+        }
+        T p1[NDIM], f[NDIM], delta[NDIM];
+        int lo[NDIM], hi[NDIM];
+#pragma unroll
+        for (int d = 0; d < NDIM; ++d) {
+            p1[d] = clamp_to_axis(following < T(1) ? a[d] + following * dl[d] : b[d], g.num[d], g.code[d]);
+            if (times[d] <= following) plane[d] += step[d];
+            linear_nodes<T>(T(0.5) * (p0[d] + p1[d]), g.num[d], g.code[d], lo[d], hi[d], f[d]);
+            delta[d] = p1[d] - p0[d];
+        }
+        if constexpr (NDIM == 1) {
+            sink.add(lo, 0, q * delta[0]);
+        } else if constexpr (NDIM == 2) {
+            const T along_x = q * delta[0];
+            const T along_y = q * delta[1];
+            int n[2];
+            n[0] = lo[0]; n[1] = lo[1]; sink.add(n, 0, (T(1) - f[1]) * along_x);
+            n[0] = lo[0]; n[1] = hi[1]; sink.add(n, 0, f[1] * along_x);
+            n[0] = lo[0]; n[1] = lo[1]; sink.add(n, 1, (T(1) - f[0]) * along_y);
+            n[0] = hi[0]; n[1] = lo[1]; sink.add(n, 1, f[0] * along_y);
+        } else {
+#pragma unroll
+            for (int axis = 0; axis < 3; ++axis) {
+                // the two axes across this one, in increasing order
+                const int ua = axis == 0 ? 1 : 0;
+                const int wa = axis == 2 ? 1 : 2;
+                const T cross = delta[ua] * delta[wa] / T(12);
+                const T along = q * delta[axis];
+#pragma unroll
+                for (int u = 0; u < 2; ++u)
+#pragma unroll
+                    for (int w = 0; w < 2; ++w) {
+                        const T eu = u ? f[ua] : T(1) - f[ua];
+                        const T ew = w ? f[wa] : T(1) - f[wa];
+                        const T weight = eu * ew + (u == w ? cross : -cross);
+                        int n[3] = {lo[0], lo[1], lo[2]};
+                        n[ua] = u ? hi[ua] : lo[ua];
+                        n[wa] = w ? hi[wa] : lo[wa];
+                        sink.add(n, axis, along * weight);
+                    }
+            }
+        }
+        time = following;
+#pragma unroll
+        for (int d = 0; d < NDIM; ++d) p0[d] = p1[d];
+    }
+}
+
+__device__ __forceinline__ int floor_to_int(double x) {
+    int whole = trunc_int<double>(x);
+    if (x < (double)whole) whole -= 1;
+    return whole;
+}
+__device__ __forceinline__ int floor_to_int(float x) {
+    int whole = trunc_int<float>(x);
+    if (x < (float)whole) whole -= 1;
+    return whole;
+}
+
+// The P edges along an axis around rel: their (mapped) first nodes, weights
+// B_{P-1}(rel - k - 1/2) and whether each exists (spline_edges.cuh:22-65).
+template <typename T, int P>
+__device__ __forceinline__ void along_stencil(T rel, int num, int code, int* edge, T* weight, bool* exists) {
+    if (code == CLAMPED) {
+        const int cell = clamped_cell<T, P, true>(rel, num, weight);
+#pragma unroll
+        for (int a = 0; a < P; ++a) {
+            edge[a] = cell + a;
+            exists[a] = true;
+        }
+        return;
+    }
+    constexpr int LOWER = P - 1;
+    if (code == PERIODIC && !(rel >= T(0) && rel < T(num))) rel = wrap_period(rel, num);
+    const T shifted = rel - T(0.5);
+    int middle;
+    if constexpr (LOWER % 2 == 0) {
+        middle = floor_to_int(shifted + T(0.5));
+        if (code == BOUNDED && middle > num - 2) middle = num - 2;
+    } else {
+        middle = floor_to_int(shifted);
+    }
+    middle = clampi(middle, -2, num + 1);
+    uniform_weights<T, LOWER>(shifted - T(middle), weight);
+    const int first = middle - LOWER / 2;
+#pragma unroll
+    for (int a = 0; a < P; ++a) {
+        const int k = first + a;
+        if (code == PERIODIC) {
+            edge[a] = map_node(k, num, PERIODIC);
+            exists[a] = true;
+        } else if (k < 0 || k > num - 2) {
+            edge[a] = 0;
+            exists[a] = false;
+        } else {
+            edge[a] = k;
+            exists[a] = true;
+        }
+    }
+}
+
+// Gauss-Legendre points and weights on [0, 1] for COUNT = 1..5 points: the values of
+// numpy.polynomial.legendre.leggauss(COUNT) mapped from [-1, 1] (spline_edges.cuh:67-89).
+template <typename T, int COUNT> struct Gauss;
+template <typename T> struct Gauss<T, 1> {
+    static __device__ __forceinline__ T point(int) { return T(0.5); }
+    static __device__ __forceinline__ T weight(int) { return T(1.0); }
+};
+template <typename T> struct Gauss<T, 2> {
+    static __device__ __forceinline__ T point(int g) { return g == 0 ? T(0.21132486540518713) : T(0.7886751345948129); }
+    static __device__ __forceinline__ T weight(int) { return T(0.5); }
+};
+template <typename T> struct Gauss<T, 3> {
+    static __device__ __forceinline__ T point(int g) {
+        return g == 0 ? T(0.1127016653792583) : (g == 1 ? T(0.5) : T(0.8872983346207417));
+    }
+    static __device__ __forceinline__ T weight(int g) {
+        return g == 1 ? T(0.4444444444444444) : T(0.2777777777777778);
+    }
+};
+template <typename T> struct Gauss<T, 4> {
+    static __device__ __forceinline__ T point(int g) {
+        const T p[4] = {T(0.06943184420297371), T(0.33000947820757187), T(0.6699905217924281), T(0.9305681557970262)};
+        return p[g];
+    }
+    static __device__ __forceinline__ T weight(int g) {
+        return (g == 0 || g == 3) ? T(0.17392742256872692) : T(0.3260725774312731);
+    }
+};
+template <typename T> struct Gauss<T, 5> {
+    static __device__ __forceinline__ T point(int g) {
+        const T p[5] = {T(0.04691007703066802), T(0.23076534494715845), T(0.5), T(0.7692346550528415), T(0.9530899229693319)};
+        return p[g];
+    }
+    static __device__ __forceinline__ T weight(int g) {
+        const T w[5] = {T(0.11846344252809454), T(0.2393143352496832), T(0.28444444444444444), T(0.2393143352496832), T(0.11846344252809454)};
+        return w[g];
+    }
+};
+
+// The ascending crossing times of one axis over a stretch: knot planes first..last
+// walked in the direction of increasing time, then merged with the two wall times.
+template <typename T> struct CutStream {
+    T a0, delta, plane;
+    int left;   // planes not yet taken
+    T stepdir;  // +1 or -1
+    T wall[2];
+    int walls;  // walls not yet taken (taken from wall[2 - walls])
+
+    __device__ __forceinline__ void init(T s0, T s1, T shift, int num, int code) {
+        a0 = s0;
+        delta = s1 - s0;
+        left = 0;
+        walls = 0;
+        plane = T(0);
+        stepdir = T(1);
+        if (delta == T(0)) return;
+        const T low = delta > T(0) ? s0 : s1;
+        const T high = delta > T(0) ? s1 : s0;
+        const T offset = code == CLAMPED ? T(0) : shift;
+        const T first = T(floor_to_int(low - offset)) + T(1) + offset;
+        int count = 0;
+        while (first + T(count) < high && count < 64) ++count;
+        left = count;
+        if (delta > T(0)) {
+            plane = first;
+            stepdir = T(1);
+        } else {
+            plane = first + T(count - 1);
+            stepdir = T(-1);
+        }
+        if (code != PERIODIC) {
+            T t0 = (T(0) - s0) / delta;
+            T t1 = (T(num) - T(1) - s0) / delta;
+            const bool in0 = t0 > T(0) && t0 < T(1);
+            const bool in1 = t1 > T(0) && t1 < T(1);
+            if (in0 && in1) {
+                wall[0] = t0 < t1 ? t0 : t1;
+                wall[1] = t0 < t1 ? t1 : t0;
+                walls = 2;
+            } else if (in0 || in1) {
+                wall[1] = in0 ? t0 : t1;
+                walls = 1;
+            }
+        }
+    }
+    // The next plane time inside (0, 1), skipping the ones rounding outside.
+    __device__ __forceinline__ T peek_plane() {
+        while (left > 0) {
+            const T t = (plane - a0) / delta;
+            if (t > T(0) && t < T(1)) return t;
+            plane += stepdir;
+            --left;
+        }
+        return T(2);
+    }
+    __device__ __forceinline__ T peek_wall() const { return walls > 0 ? wall[2 - walls] : T(2); }
+};
+
+template <typename T, int NDIM, int P, typename Sink>
+__device__ void spline_path(T q, const T* r0, const T* r1, const Grid<T>& g, const Sink& sink) {
+    constexpr int NPTS = (P - 1 + (NDIM - 1) * P) / 2 + 1;
+    const T shift = (P % 2 == 0) ? T(0.5) : T(0);
+    T extent = T(0);
+#pragma unroll
+    for (int d = 0; d < NDIM; ++d) {
+        const T span = r1[d] > r0[d] ? r1[d] - r0[d] : r0[d] - r1[d];
+        if (span > extent) extent = span;
+    }
+    int stretches = trunc_int<T>(extent / T(4)) + 1;
+    if (stretches > kMaxPathSteps || stretches < 1) stretches = kMaxPathSteps;
+    for (int st = 0; st < stretches; ++st) {
+        T a0[NDIM], a1[NDIM];
+        CutStream<T> cs[NDIM];
+#pragma unroll
+        for (int d = 0; d < NDIM; ++d) {
+            a0[d] = r0[d] + (r1[d] - r0[d]) * T(st) / T(stretches);
+            a1[d] = r0[d] + (r1[d] - r0[d]) * T(st + 1) / T(stretches);
+            cs[d].init(a0[d], a1[d], shift, g.num[d], g.code[d]);
+        }
+        T t0 = T(0);
+        for (int guard = 0; guard < 64; ++guard) {
+            // the next cut: the least pending time of every stream, or the end
+            T t1 = T(1);
+            int which = -1;
+#pragma unroll
+            for (int d = 0; d < NDIM; ++d) {
+                const T tp = cs[d].peek_plane();
+                if (tp < t1) { t1 = tp; which = 2 * d; }
+                const T tw = cs[d].peek_wall();
+                if (tw < t1) { t1 = tw; which = 2 * d + 1; }
+            }
+            if (which >= 0) {
+#pragma unroll
+                for (int d = 0; d < NDIM; ++d) {
+                    if (which == 2 * d) { cs[d].plane += cs[d].stepdir; --cs[d].left; }
+                    if (which == 2 * d + 1) --cs[d].walls;
+                }
+            }
+            if (t1 > t0) {
+                T p0[NDIM], step[NDIM];
+#pragma unroll
+                for (int d = 0; d < NDIM; ++d) {
+                    T begin = a0[d] + t0 * (a1[d] - a0[d]);
+                    T finish = a0[d] + t1 * (a1[d] - a0[d]);
+                    if (g.code[d] != PERIODIC) {
+                        const T top = T(g.num[d] - 1);
+                        if (begin < T(0)) begin = T(0);
+                        if (begin > top) begin = top;
+                        if (finish < T(0)) finish = T(0);
+                        if (finish > top) finish = top;
+                    }
+                    p0[d] = begin;
+                    step[d] = finish - begin;
+                }
+#pragma unroll
+                for (int gp = 0; gp < NPTS; ++gp) {
+                    const T point = Gauss<T, NPTS>::point(gp);
+                    const T gw = Gauss<T, NPTS>::weight(gp);
+                    T rel[NDIM];
+#pragma unroll
+                    for (int d = 0; d < NDIM; ++d) rel[d] = p0[d] + point * step[d];
+#pragma unroll
+                    for (int axis = 0; axis < NDIM; ++axis) {
+                        const T amount = q * gw * step[axis];
+                        if (amount == T(0)) continue;
+                        int idx[3][P + 1];
+                        T wt[3][P + 1];
+                        bool ex[P > 0 ? P : 1];
+#pragma unroll
+                        for (int d = 0; d < NDIM; ++d) {
+                            if (d == axis) {
+                                along_stencil<T, P>(rel[d], g.num[d], g.code[d], idx[d], wt[d], ex);
+                            } else {
+                                const int base = axis_stencil<T, SPLINE, P>(rel[d], g.num[d], g.code[d], wt[d]);
+#pragma unroll
+                                for (int s = 0; s <= P; ++s) idx[d][s] = map_node(base + s, g.num[d], g.code[d]);
+                            }
+                        }
+                        constexpr int SX = P + 1;
+                        const int cnt0 = axis == 0 ? P : SX;
+                        const int cnt1 = NDIM > 1 ? (axis == 1 ? P : SX) : 1;
+                        const int cnt2 = NDIM > 2 ? (axis == 2 ? P : SX) : 1;
+                        for (int x = 0; x < cnt0; ++x) {
+                            if (axis == 0 && !ex[x]) continue;
+                            for (int y = 0; y < cnt1; ++y) {
+                                if (NDIM > 1 && axis == 1 && !ex[y]) continue;
+                                for (int z = 0; z < cnt2; ++z) {
+                                    if (NDIM > 2 && axis == 2 && !ex[z]) continue;
+                                    T w = amount * wt[0][x];
+                                    if constexpr (NDIM > 1) w = w * wt[1][y];
+                                    if constexpr (NDIM > 2) w = w * wt[2][z];
+                                    int n[3] = {idx[0][x], NDIM > 1 ? idx[1][y] : 0, NDIM > 2 ? idx[2][z] : 0};
+                                    sink.add(n, axis, w);
+                                }
+                            }
+                        }
+                    }
+                }
+                t0 = t1;
+            }
+            if (which < 0) break;
+        }
+    }
+}
+
+// One thread per path, global atomics.
+template <typename T, int NDIM, int P, bool WHITNEY>
+__global__ void __launch_bounds__(256) deposit_paths_kernel(const PathArgs<T> a) {
+    GlobalEdgeSink<T, NDIM> sink;
+    sink.edges = a.edges_out;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) sink.ext[d] = a.g.ext[d];
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const T q = a.charges[i];
+        if (q == T(0)) continue;
+        T r0[NDIM], r1[NDIM];
+        bool finite = true;
+#pragma unroll
+        for (int d = 0; d < NDIM; ++d) {
+            const T s = a.start[d * a.start_stride + i];
+            const T e = a.end[d * a.end_stride + i];
+            r0[d] = (s - a.g.lower[d]) / a.g.cell[d];
+            r1[d] = (e - a.g.lower[d]) / a.g.cell[d];
+            if constexpr (WHITNEY) {
+                const T big = sizeof(T) == 8 ? T(1e300) : T(3e38);
+                if (!(r0[d] > -big && r0[d] < big && r1[d] > -big && r1[d] < big)) finite = false;
+            } else {
+                if (!(s - s == T(0)) || !(e - e == T(0))) finite = false;
+            }
+        }
+        if (!finite) continue;
+        if constexpr (WHITNEY) whitney_path<T, NDIM>(q, r0, r1, a.g, sink);
+        else spline_path<T, NDIM, P>(q, r0, r1, a.g, sink);
+    }
+}
+
+// The field of an edge field at the markers (gather_edges_{1,2,3}d for WHITNEY,
+// gather_edges_spline_{1,2,3}d for the spline edges), divided by the cell size.
+template <typename T, int NDIM, int P, bool WHITNEY>
+__global__ void __launch_bounds__(256) gather_edges_kernel(const PathArgs<T> a) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        T rel[NDIM];
+#pragma unroll
+        for (int d = 0; d < NDIM; ++d) {
+            rel[d] = (a.pos[d * a.pos_stride + i] - a.g.lower[d]) / a.g.cell[d];
+            if (!WHITNEY && a.g.code[d] != PERIODIC) {
+                const T top = T(a.g.num[d] - 1);
+                if (rel[d] < T(0)) rel[d] = T(0);
+                if (rel[d] > top) rel[d] = top;
+            }
+        }
+#pragma unroll
+        for (int axis = 0; axis < NDIM; ++axis) {
+            constexpr int S = WHITNEY ? 2 : P + 1;
+            int idx[3][S];
+            T wt[3][S];
+            bool ex[S];
+            int cnt[3] = {1, 1, 1};
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                idx[d][0] = 0;
+                wt[d][0] = T(1);
+            }
+#pragma unroll
+            for (int s = 0; s < S; ++s) ex[s] = true;
+#pragma unroll
+            for (int d = 0; d < NDIM; ++d) {
+                if constexpr (WHITNEY) {
+                    int lo, hi;
+                    T f;
+                    linear_nodes<T>(rel[d], a.g.num[d], a.g.code[d], lo, hi, f);
+                    if (d == axis) {
+                        idx[d][0] = lo;
+                        wt[d][0] = T(1);
+                        cnt[d] = 1;
+                    } else {
+                        idx[d][0] = lo;
+                        idx[d][1] = hi;
+                        wt[d][0] = T(1) - f;
+                        wt[d][1] = f;
+                        cnt[d] = 2;
+                    }
+                } else {
+                    if (d == axis) {
+                        along_stencil<T, P>(rel[d], a.g.num[d], a.g.code[d], idx[d], wt[d], ex);
+                        cnt[d] = P;
+                    } else {
+                        const int base = axis_stencil<T, SPLINE, P>(rel[d], a.g.num[d], a.g.code[d], wt[d]);
+#pragma unroll
+                        for (int s = 0; s <= P; ++s) idx[d][s] = map_node(base + s, a.g.num[d], a.g.code[d]);
+                        cnt[d] = P + 1;
+                    }
+                }
+            }
+            T total = T(0);
+            for (int x = 0; x < cnt[0]; ++x) {
+                if (axis == 0 && !ex[x]) continue;
+                for (int y = 0; y < cnt[1]; ++y) {
+                    if (axis == 1 && !ex[y]) continue;
+                    for (int z = 0; z < cnt[2]; ++z) {
+                        if (axis == 2 && !ex[z]) continue;
+                        T w = wt[0][x];
+                        if (NDIM > 1) w = w * wt[1][y];
+                        if (NDIM > 2) w = w * wt[2][z];
+                        int64_t k = idx[0][x];
+                        if (NDIM > 1) k = k * a.g.ext[1] + idx[1][y];
+                        if (NDIM > 2) k = k * a.g.ext[2] + idx[2][z];
+                        total += w * __ldg(a.edges_in + k * NDIM + axis);
+                    }
+                }
+            }
+            a.result[axis * a.res_stride + i] = total / a.g.cell[axis];
+        }
+    }
+}
+
+}  // namespace mpf

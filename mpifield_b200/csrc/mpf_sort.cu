@@ -1,0 +1,372 @@
+// mpf_sort.cu -- the cell-tile keys of the markers and their stable sort.
+//
+// The key of a marker is the tile of the anchor node of its stencil (mpf_stencil.cuh,
+// axis_anchor), row-major over the tiles; a marker whose values are all zero gets the
+// sentinel key num_tiles without its position being read. The sort is a least-
+// significant-digit radix sort of (key, marker) pairs with 8-bit digits, as many passes
+// as the key needs bits. Each pass: a per-CTA digit histogram, an exclusive scan of the
+// histograms in digit-major order, and a stable scatter in which every warp ranks its
+// 32 keys of a round with __match_any_sync against a per-warp digit count, so the rank
+// of a key follows the marker order inside the warp, the warps of a CTA and the CTAs:
+// the result is the stable order (numpy.argsort(keys, kind="stable")), bit for bit.
+#include <algorithm>
+#include <cstdint>
+
+#include "mpf_internal.h"
+#include "mpf_stencil.cuh"
+#include "mpifield_b200.h"
+
+namespace mpf {
+
+constexpr int kSortBlock = 256;
+constexpr int kSortItems = 16;  // keys per thread per tile
+constexpr int kSortTile = kSortBlock * kSortItems;
+constexpr int kDigits = 256;
+constexpr int kWarps = kSortBlock / 32;
+
+
+template <typename T, int NDIM, int KIND, int P>
+__global__ void tile_keys_kernel(const KeyArgs<T> a) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        if (a.values) {
+            bool live = false;
+            for (int64_t c = 0; c < a.ncomp; ++c) live = live || a.values[c * a.val_stride + i] != T(0);
+            if (!live) {
+                a.keys[i] = a.sentinel;
+                continue;
+            }
+        }
+        int64_t key = 0;
+#pragma unroll
+        for (int d = 0; d < NDIM; ++d) {
+            const T rel = (a.pos[d * a.pos_stride + i] - a.g.lower[d]) / a.g.cell[d];
+            const int anchor = axis_anchor<T, KIND, P>(rel, a.g.num[d], a.g.code[d]);
+            key = key * a.ntiles[d] + anchor / a.tile[d];
+        }
+        a.keys[i] = (uint32_t)key;
+    }
+}
+
+__global__ void digit_histogram_kernel(const uint32_t* keys, int64_t n, int shift, uint32_t* counts,
+                                       int64_t nblocks) {
+    __shared__ uint32_t hist[kDigits];
+    for (int d = threadIdx.x; d < kDigits; d += blockDim.x) hist[d] = 0;
+    __syncthreads();
+    const int64_t base = (int64_t)blockIdx.x * kSortTile;
+    for (int k = threadIdx.x; k < kSortTile; k += blockDim.x) {
+        const int64_t i = base + k;
+        if (i < n) atomicAdd(&hist[(keys[i] >> shift) & 0xff], 1u);
+    }
+    __syncthreads();
+    for (int d = threadIdx.x; d < kDigits; d += blockDim.x) counts[(int64_t)d * nblocks + blockIdx.x] = hist[d];
+}
+
+// Exclusive scan of `count` u32 values in place, in three kernels: chunk sums, a scan of
+// the sums in one CTA, and the chunks rescanned with their offsets.
+constexpr int kScanChunk = 2048;
+
+__global__ void scan_sums_kernel(const uint32_t* data, int64_t count, uint32_t* sums) {
+    __shared__ uint32_t part[kSortBlock / 32];
+    const int64_t base = (int64_t)blockIdx.x * kScanChunk;
+    uint32_t s = 0;
+    for (int k = threadIdx.x; k < kScanChunk; k += blockDim.x) {
+        const int64_t i = base + k;
+        if (i < count) s += data[i];
+    }
+    s = __reduce_add_sync(0xffffffffu, s);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += part[w];
+        sums[blockIdx.x] = t;
+    }
+}
+
+__global__ void scan_single_kernel(uint32_t* sums, int64_t count) {
+    // one CTA: sequential over chunks of blockDim, scan within each
+    __shared__ uint32_t buf[kSortBlock];
+    __shared__ uint32_t carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int64_t base = 0; base < count; base += blockDim.x) {
+        const int64_t i = base + threadIdx.x;
+        const uint32_t v = i < count ? sums[i] : 0;
+        buf[threadIdx.x] = v;
+        __syncthreads();
+        for (int off = 1; off < (int)blockDim.x; off <<= 1) {
+            const uint32_t add = threadIdx.x >= (unsigned)off ? buf[threadIdx.x - off] : 0;
+            __syncthreads();
+            buf[threadIdx.x] += add;
+            __syncthreads();
+        }
+        if (i < count) sums[i] = carry + buf[threadIdx.x] - v;
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) carry += buf[threadIdx.x];
+        __syncthreads();
+    }
+}
+
+__global__ void scan_chunks_kernel(uint32_t* data, int64_t count, const uint32_t* offsets) {
+    __shared__ uint32_t buf[kSortBlock];
+    __shared__ uint32_t carry;
+    const int64_t base = (int64_t)blockIdx.x * kScanChunk;
+    if (threadIdx.x == 0) carry = offsets[blockIdx.x];
+    __syncthreads();
+    for (int sub = 0; sub < kScanChunk; sub += blockDim.x) {
+        const int64_t i = base + sub + threadIdx.x;
+        const uint32_t v = i < count ? data[i] : 0;
+        buf[threadIdx.x] = v;
+        __syncthreads();
+        for (int off = 1; off < (int)blockDim.x; off <<= 1) {
+            const uint32_t add = threadIdx.x >= (unsigned)off ? buf[threadIdx.x - off] : 0;
+            __syncthreads();
+            buf[threadIdx.x] += add;
+            __syncthreads();
+        }
+        if (i < count) data[i] = carry + buf[threadIdx.x] - v;
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) carry += buf[threadIdx.x];
+        __syncthreads();
+    }
+}
+
+// The stable scatter of one pass. Warp w of a CTA owns the contiguous segment
+// [w * 32 * kSortItems, (w + 1) * 32 * kSortItems) of the CTA's tile and walks it in
+// rounds of 32 consecutive keys.
+__global__ void digit_scatter_kernel(const uint32_t* keys_in, const int32_t* vals_in, int64_t n,
+                                     int shift, const uint32_t* offsets, int64_t nblocks,
+                                     uint32_t* keys_out, int32_t* vals_out) {
+    __shared__ uint32_t warp_count[kWarps][kDigits];
+    __shared__ uint32_t warp_base[kWarps][kDigits];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    for (int d = threadIdx.x; d < kWarps * kDigits; d += blockDim.x) (&warp_count[0][0])[d] = 0;
+    __syncthreads();
+    const int64_t seg = (int64_t)blockIdx.x * kSortTile + (int64_t)warp * 32 * kSortItems;
+    uint32_t key[kSortItems];
+    int32_t val[kSortItems];
+    uint32_t rank[kSortItems];
+    const unsigned below = (1u << lane) - 1u;
+#pragma unroll
+    for (int r = 0; r < kSortItems; ++r) {
+        const int64_t i = seg + (int64_t)r * 32 + lane;
+        const bool have = i < n;
+        key[r] = have ? keys_in[i] : 0xffffffffu;
+        val[r] = have ? (vals_in ? vals_in[i] : (int32_t)i) : 0;
+        const uint32_t digit = (key[r] >> shift) & 0xff;
+        // lanes holding the same digit this round, and those of them before this lane
+        const unsigned same = __match_any_sync(0xffffffffu, have ? (int)digit : -1 - lane);
+        const unsigned before = __popc(same & below);
+        const uint32_t count = have ? warp_count[warp][digit] : 0;
+        rank[r] = count + before;
+        __syncwarp();
+        if (have && before == 0) warp_count[warp][digit] = count + __popc(same);
+        __syncwarp();
+    }
+    __syncthreads();
+    // the offset of every warp's digit run inside the CTA, then in the whole array
+    for (int d = threadIdx.x; d < kDigits; d += blockDim.x) {
+        uint32_t s = offsets[(int64_t)d * nblocks + blockIdx.x];
+        for (int w = 0; w < kWarps; ++w) {
+            warp_base[w][d] = s;
+            s += warp_count[w][d];
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < kSortItems; ++r) {
+        const int64_t i = seg + (int64_t)r * 32 + lane;
+        if (i < n) {
+            const uint32_t digit = (key[r] >> shift) & 0xff;
+            const uint32_t dst = warp_base[warp][digit] + rank[r];
+            keys_out[dst] = key[r];
+            vals_out[dst] = val[r];
+        }
+    }
+}
+
+// tile_start[k] = the first rank whose key is >= k, k = 0 .. num_tiles; tile_start[num_tiles + 1] = n.
+__global__ void tile_starts_kernel(const uint32_t* sorted, int64_t n, int64_t num_tiles, int64_t* start) {
+    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j <= n;
+         j += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t prev = j == 0 ? -1 : (int64_t)sorted[j - 1];
+        const int64_t cur = j == n ? num_tiles + 1 : (int64_t)sorted[j];
+        for (int64_t k = prev + 1; k <= cur && k <= num_tiles + 1; ++k) start[k] = (k == num_tiles + 1) ? n : j;
+    }
+}
+
+template <typename T>
+__global__ void permute_rows_kernel(T* dst, int64_t ds, const T* src, int64_t ss, int64_t rows,
+                                    const int32_t* order, int64_t n) {
+    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n;
+         j += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t from = order[j];
+        // an order entry outside [0, n) reads nothing: the row gets NaN
+        const bool inside = from >= 0 && from < n;
+        for (int64_t r = 0; r < rows; ++r) dst[r * ds + j] = inside ? __ldg(src + r * ss + from) : T(NAN);
+    }
+}
+
+template <typename T>
+__global__ void unpermute_rows_kernel(T* dst, int64_t ds, const T* src, int64_t ss, int64_t rows,
+                                      const int32_t* order, int64_t n) {
+    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n;
+         j += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t to = order[j];
+        if (to < 0 || to >= n) continue;  // an entry outside [0, n) writes nothing
+        for (int64_t r = 0; r < rows; ++r) dst[r * ds + to] = src[r * ss + j];
+    }
+}
+
+// ------------------------------------------------------------------ host side --
+
+static int64_t sort_blocks(int64_t n) { return std::max<int64_t>(1, (n + kSortTile - 1) / kSortTile); }
+static int64_t scan_chunks(int64_t count) { return std::max<int64_t>(1, (count + kScanChunk - 1) / kScanChunk); }
+static size_t align256(size_t b) { return (b + 255) / 256 * 256; }
+
+struct SortLayout {
+    size_t keys_a, keys_b, vals_a, vals_b, counts, sums, total;
+};
+
+static SortLayout sort_layout(int64_t n) {
+    SortLayout L;
+    const int64_t nb = sort_blocks(n);
+    const int64_t count = nb * kDigits;
+    size_t off = 0;
+    L.keys_a = off; off += align256(sizeof(uint32_t) * std::max<int64_t>(n, 1));
+    L.keys_b = off; off += align256(sizeof(uint32_t) * std::max<int64_t>(n, 1));
+    L.vals_a = off; off += align256(sizeof(int32_t) * std::max<int64_t>(n, 1));
+    L.vals_b = off; off += align256(sizeof(int32_t) * std::max<int64_t>(n, 1));
+    L.counts = off; off += align256(sizeof(uint32_t) * count);
+    L.sums = off; off += align256(sizeof(uint32_t) * scan_chunks(count));
+    L.total = off;
+    return L;
+}
+
+size_t sort_workspace_bytes(int64_t n) { return sort_layout(n).total; }
+
+static int scan_exclusive(uint32_t* data, int64_t count, uint32_t* sums, cudaStream_t stream) {
+    const int64_t chunks = scan_chunks(count);
+    scan_sums_kernel<<<(unsigned)chunks, kSortBlock, 0, stream>>>(data, count, sums);
+    count_launches(1);
+    scan_single_kernel<<<1, kSortBlock, 0, stream>>>(sums, chunks);
+    count_launches(1);
+    scan_chunks_kernel<<<(unsigned)chunks, kSortBlock, 0, stream>>>(data, count, sums);
+    count_launches(1);
+    return cudaGetLastError() == cudaSuccess ? MPF_OK : MPF_ERR_CUDA;
+}
+
+template <typename T, int NDIM, int KIND, int P>
+static int run_keys(const KeyArgs<T>& a, cudaStream_t stream) {
+    const int block = 256;
+    const int64_t blocks = std::min<int64_t>((a.n + block - 1) / block, (int64_t)sm_count() * 16);
+    tile_keys_kernel<T, NDIM, KIND, P><<<(unsigned)std::max<int64_t>(blocks, 1), block, 0, stream>>>(a);
+    count_launches(1);
+    return cudaGetLastError() == cudaSuccess ? MPF_OK : MPF_ERR_CUDA;
+}
+
+template <typename T, int NDIM>
+static int keys_by_kind(int kind, int degree, const KeyArgs<T>& a, cudaStream_t stream) {
+    if (kind == LINEAR) return run_keys<T, NDIM, LINEAR, 1>(a, stream);
+    if (kind == QUADRATIC) return run_keys<T, NDIM, QUADRATIC, 2>(a, stream);
+    switch (degree) {
+        case 0: return run_keys<T, NDIM, SPLINE, 0>(a, stream);
+        case 1: return run_keys<T, NDIM, SPLINE, 1>(a, stream);
+        case 2: return run_keys<T, NDIM, SPLINE, 2>(a, stream);
+        case 3: return run_keys<T, NDIM, SPLINE, 3>(a, stream);
+    }
+    return MPF_ERR_ARGUMENT;
+}
+
+template <typename T>
+int tile_keys(int kind, int degree, int ndim, const KeyArgs<T>& a, cudaStream_t stream) {
+    switch (ndim) {
+        case 1: return keys_by_kind<T, 1>(kind, degree, a, stream);
+        case 2: return keys_by_kind<T, 2>(kind, degree, a, stream);
+        case 3: return keys_by_kind<T, 3>(kind, degree, a, stream);
+    }
+    return MPF_ERR_ARGUMENT;
+}
+
+// Sort (keys, marker) pairs stably; the marker order lands in `order`, the tile starts
+// in `tile_start`.
+int sort_keys(const uint32_t* keys, int64_t n, int64_t num_tiles, int32_t* order, int64_t* tile_start,
+              void* workspace, cudaStream_t stream) {
+    if (n == 0) {
+        tile_starts_kernel<<<1, 256, 0, stream>>>(nullptr, 0, num_tiles, tile_start);
+        count_launches(1);
+        return cudaGetLastError() == cudaSuccess ? MPF_OK : MPF_ERR_CUDA;
+    }
+    const SortLayout L = sort_layout(n);
+    char* ws = static_cast<char*>(workspace);
+    uint32_t* ka = reinterpret_cast<uint32_t*>(ws + L.keys_a);
+    uint32_t* kb = reinterpret_cast<uint32_t*>(ws + L.keys_b);
+    int32_t* va = reinterpret_cast<int32_t*>(ws + L.vals_a);
+    int32_t* vb = reinterpret_cast<int32_t*>(ws + L.vals_b);
+    uint32_t* counts = reinterpret_cast<uint32_t*>(ws + L.counts);
+    uint32_t* sums = reinterpret_cast<uint32_t*>(ws + L.sums);
+    int bits = 1;
+    while (bits < 32 && ((uint64_t)num_tiles >> bits) != 0) ++bits;  // the sentinel num_tiles included
+    const int passes = std::max(1, (bits + 7) / 8);
+    const int64_t nb = sort_blocks(n);
+    const uint32_t* kin = keys;
+    const int32_t* vin = nullptr;  // the first pass numbers the markers itself
+    uint32_t* kout_buf[2] = {ka, kb};
+    int32_t* vout_buf[2] = {va, vb};
+    uint32_t* kout = ka;
+    for (int p = 0; p < passes; ++p) {
+        const int shift = 8 * p;
+        kout = kout_buf[p & 1];
+        int32_t* vout = (p == passes - 1) ? order : vout_buf[p & 1];
+        digit_histogram_kernel<<<(unsigned)nb, kSortBlock, 0, stream>>>(kin, n, shift, counts, nb);
+        count_launches(1);
+        if (cudaGetLastError() != cudaSuccess) return MPF_ERR_CUDA;
+        int st = scan_exclusive(counts, nb * kDigits, sums, stream);
+        if (st != MPF_OK) return st;
+        digit_scatter_kernel<<<(unsigned)nb, kSortBlock, 0, stream>>>(kin, vin, n, shift, counts, nb, kout, vout);
+        count_launches(1);
+        if (cudaGetLastError() != cudaSuccess) return MPF_ERR_CUDA;
+        kin = kout;
+        vin = vout;
+    }
+    const int block = 256;
+    const int64_t blocks = std::min<int64_t>((n + 1 + block - 1) / block, (int64_t)sm_count() * 16);
+    tile_starts_kernel<<<(unsigned)std::max<int64_t>(blocks, 1), block, 0, stream>>>(kout, n, num_tiles, tile_start);
+    count_launches(1);
+    return cudaGetLastError() == cudaSuccess ? MPF_OK : MPF_ERR_CUDA;
+}
+
+int permute_rows(void* dst, int64_t ds, const void* src, int64_t ss, int64_t rows, const int32_t* order,
+                 int64_t n, int dtype, cudaStream_t stream) {
+    const int block = 256;
+    const int64_t blocks = std::min<int64_t>((n + block - 1) / block, (int64_t)sm_count() * 16);
+    if (dtype == MPF_F64)
+        permute_rows_kernel<double><<<(unsigned)std::max<int64_t>(blocks, 1), block, 0, stream>>>(
+            (double*)dst, ds, (const double*)src, ss, rows, order, n);
+    else
+        permute_rows_kernel<float><<<(unsigned)std::max<int64_t>(blocks, 1), block, 0, stream>>>(
+            (float*)dst, ds, (const float*)src, ss, rows, order, n);
+    count_launches(1);
+    return cudaGetLastError() == cudaSuccess ? MPF_OK : MPF_ERR_CUDA;
+}
+
+int unpermute_rows(void* dst, int64_t ds, const void* src, int64_t ss, int64_t rows, const int32_t* order,
+                   int64_t n, int dtype, cudaStream_t stream) {
+    const int block = 256;
+    const int64_t blocks = std::min<int64_t>((n + block - 1) / block, (int64_t)sm_count() * 16);
+    if (dtype == MPF_F64)
+        unpermute_rows_kernel<double><<<(unsigned)std::max<int64_t>(blocks, 1), block, 0, stream>>>(
+            (double*)dst, ds, (const double*)src, ss, rows, order, n);
+    else
+        unpermute_rows_kernel<float><<<(unsigned)std::max<int64_t>(blocks, 1), block, 0, stream>>>(
+            (float*)dst, ds, (const float*)src, ss, rows, order, n);
+    count_launches(1);
+    return cudaGetLastError() == cudaSuccess ? MPF_OK : MPF_ERR_CUDA;
+}
+
+template int tile_keys<double>(int, int, int, const KeyArgs<double>&, cudaStream_t);
+template int tile_keys<float>(int, int, int, const KeyArgs<float>&, cudaStream_t);
+
+}  // namespace mpf

@@ -1,0 +1,111 @@
+"""Cell-tile sort of markers: keys, a stable order and the start of every tile.
+
+Markers sorted by cell tile are what the shared-memory boxes of the gather and scatter
+kernels need (each chunk of markers then touches one small box of the grid). The key of
+a marker is the tile of its stencil's anchor node (the node LINEAR, QUADRATIC or the
+spline stencil is anchored on), row-major over tiles of ``tile`` nodes per axis; a
+marker whose values are all zero goes to the sentinel tile ``num_tiles`` without its
+position being read. The order is stable: equal keys keep the marker order, so the
+result equals ``numpy.argsort(keys, kind="stable")`` bit for bit. The workspace is
+allocated here by torch and passed to the C call, which allocates nothing.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import torch
+
+from mpifield_b200 import _lib
+from mpifield_b200.kernels import _marker_rows
+
+
+@dataclass
+class TileOrder:
+    """The result of `sort_by_tile`."""
+
+    keys: torch.Tensor        # (N,) int32 view of the uint32 keys, in marker order
+    order: torch.Tensor       # (N,) int32: the marker of every rank
+    tile_start: torch.Tensor  # (num_tiles + 2,) int64: first rank of every key, then N
+    num_tiles: int
+
+
+def _kind_of(weighting) -> tuple[int, int]:
+    """(kind, degree) of a built-in weighting, or of a ``(kind, degree)`` pair."""
+    if isinstance(weighting, tuple):
+        return int(weighting[0]), int(weighting[1])
+    kernel = weighting.gather_kernel(1)
+    return int(kernel.kind), int(kernel.fixed_degree)
+
+
+def num_tiles(weighting, geometry, tile) -> int:
+    kind, degree = _kind_of(weighting)
+    _, _, num, code, ndim = _lib.geometry_arrays(geometry)
+    t = (C.c_int32 * ndim)(*(int(v) for v in tile))
+    out = C.c_int64(0)
+    _lib.check(_lib.library().mpf_num_tiles(kind, degree, ndim, num, code, t, C.byref(out)), "num_tiles")
+    return int(out.value)
+
+
+def sort_by_tile(positions: torch.Tensor, weighting, geometry, tile, values: torch.Tensor | None = None) -> TileOrder:
+    """Sort markers by cell tile (see the module docstring)."""
+    kind, degree = _kind_of(weighting)
+    lower, cell, num, code, ndim = _lib.geometry_arrays(geometry)
+    device = _lib.require_cuda(positions)
+    dtype = positions.dtype
+    pos, ps = _marker_rows(positions, ndim, "positions", dtype)
+    n = pos.shape[1]
+    ntiles = num_tiles((kind, degree), geometry, tile)
+    t = (C.c_int32 * ndim)(*(int(v) for v in tile))
+    size = C.c_size_t(0)
+    _lib.check(_lib.library().mpf_sort_workspace_bytes(n, ntiles, C.byref(size)), "sort_workspace_bytes")
+    workspace = torch.empty(max(int(size.value), 256), dtype=torch.uint8, device=device)
+    keys = torch.empty(n, dtype=torch.int32, device=device)
+    order = torch.empty(n, dtype=torch.int32, device=device)
+    tile_start = torch.empty(ntiles + 2, dtype=torch.int64, device=device)
+    if values is not None:
+        vals, vs = _marker_rows(values, values.shape[0] if values.dim() == 2 else 1, "values", dtype)
+        vptr, ncomp = vals.data_ptr(), vals.shape[0]
+    else:
+        vptr, vs, ncomp = None, 0, 0
+    status = _lib.library().mpf_sort_by_tile(
+        kind, degree, ndim, pos.data_ptr(), ps, vptr, vs, ncomp, n, lower, cell, num, code, t,
+        keys.data_ptr(), order.data_ptr(), tile_start.data_ptr(), workspace.data_ptr(), workspace.numel(),
+        _lib.dtype_code(dtype), _lib.stream_of(device))
+    _lib.check(status, "sort_by_tile")
+    return TileOrder(keys, order, tile_start, ntiles)
+
+
+def permute(array: torch.Tensor, order: torch.Tensor) -> torch.Tensor:
+    """``array[:, order]`` for a marker array (rows, N), by the backend's permute kernel."""
+    device = _lib.require_cuda(array, order)
+    squeeze = array.dim() == 1
+    rows = 1 if squeeze else array.shape[0]
+    src, ss = _marker_rows(array, rows, "array", array.dtype)
+    n = src.shape[1]
+    dst = torch.empty((rows, n), dtype=array.dtype, device=device)
+    order = order.to(torch.int32).contiguous()
+    status = _lib.library().mpf_permute_rows(dst.data_ptr(), n, src.data_ptr(), ss, rows, order.data_ptr(), n,
+                                            _lib.dtype_code(array.dtype), _lib.stream_of(device))
+    _lib.check(status, "permute_rows")
+    return dst[0] if squeeze else dst
+
+
+def unpermute(array: torch.Tensor, order: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:
+    """The inverse of `permute`: ``out[:, order] = array`` (results back in marker order)."""
+    device = _lib.require_cuda(array, order)
+    squeeze = array.dim() == 1
+    rows = 1 if squeeze else array.shape[0]
+    src, ss = _marker_rows(array, rows, "array", array.dtype)
+    n = src.shape[1]
+    dst = out if out is not None else torch.empty((rows, n), dtype=array.dtype, device=device)
+    if dst.dim() == 1:
+        dst = dst.view(1, -1)
+    if not dst.is_contiguous() or tuple(dst.shape) != (rows, n):
+        raise ValueError(f"out must be a contiguous ({rows}, {n}) tensor")
+    order = order.to(torch.int32).contiguous()
+    status = _lib.library().mpf_unpermute_rows(dst.data_ptr(), n, src.data_ptr(), ss, rows, order.data_ptr(), n,
+                                              _lib.dtype_code(array.dtype), _lib.stream_of(device))
+    _lib.check(status, "unpermute_rows")
+    return dst[0] if squeeze else dst
