@@ -79,6 +79,9 @@ MPF_API int mpf_version(void);
 /* The number of kernels this library has launched in the process (a diagnostic). */
 MPF_API int64_t mpf_launch_count(void);
 
+/* The name of the last CUDA error behind an MPF_ERR_CUDA status ("none" if there was none). */
+MPF_API const char* mpf_last_error(void);
+
 /* A static, human-readable name of a status code. */
 MPF_API const char* mpf_status_string(int status);
 
@@ -177,24 +180,27 @@ MPF_API int mpf_add_density(void* dst, const void* deposit, int ndim, const int3
                     void* stream);
 
 /*
- * Cell-tile sort. keys[i] is the tile of marker i: the anchor node of its stencil per
- * axis (LINEAR's left node, QUADRATIC's nearest node, the middle node of a spline
- * stencil, the cell on a clamped axis) divided by tile[d], row-major over the
- * ceil(extent / tile) tiles. With `values` non-NULL ((ncomp, n) rows) a marker whose
- * values are all zero gets the key `num_tiles` without its position being read.
- * order[j] is the marker of rank j in the stable ascending order of the keys (equal to
+ * Cell-tile sort. The tile of marker i is the anchor node of its stencil per axis
+ * (LINEAR's left node, QUADRATIC's nearest node, the middle node of a spline stencil,
+ * the cell on a clamped axis) divided by tile[d], row-major over the ceil(extent / tile)
+ * tiles; keys[i] is that tile, or with `within` = 1 the tile followed by the anchor's
+ * cell inside the tile (row-major): tile * prod(tile) + cell. With `values` non-NULL
+ * ((ncomp, n) rows) a marker whose values are all zero gets the largest key (num_tiles,
+ * times prod(tile) with `within`) without its position being read. order[j] is the
+ * marker of rank j in the stable ascending order of the keys (equal to
  * numpy.argsort(keys, kind="stable")); tile_start (num_tiles + 2 entries) the first rank
- * of every key and the count n at the end. `workspace` holds `mpf_sort_workspace_bytes`
- * bytes of device memory. No reference kernel sorts (picnic's sort_by_cell is external,
+ * of every tile, of the dead markers, and n at the end. `workspace` holds
+ * `mpf_sort_workspace_bytes` bytes of device memory, 256-byte aligned. No reference
+ * kernel sorts (picnic's sort_by_cell is external,
  * src/mpifield/kernels/scatter_linear_3d/scatter_linear_3d_pyccel.py:11-12).
  */
 MPF_API int mpf_sort_workspace_bytes(int64_t n, int64_t num_tiles, size_t* bytes);
 MPF_API int mpf_sort_by_tile(int kind, int degree, int ndim, const void* positions, int64_t pos_stride,
                      const void* values, int64_t val_stride, int64_t ncomp, int64_t n,
                      const double* lower, const double* cell, const int32_t* num,
-                     const int32_t* code, const int32_t* tile, uint32_t* keys, int32_t* order,
-                     int64_t* tile_start, void* workspace, size_t workspace_bytes, int dtype,
-                     void* stream);
+                     const int32_t* code, const int32_t* tile, int within, uint32_t* keys,
+                     int32_t* order, int64_t* tile_start, void* workspace, size_t workspace_bytes,
+                     int dtype, void* stream);
 
 /* The number of tiles of a grid for mpf_sort_by_tile, into *num_tiles. */
 MPF_API int mpf_num_tiles(int kind, int degree, int ndim, const int32_t* num, const int32_t* code,

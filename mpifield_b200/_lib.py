@@ -46,6 +46,7 @@ _L = C.c_int64
 _SIGNATURES = {
     "mpf_version": ([], _I),
     "mpf_launch_count": ([], _L),
+    "mpf_last_error": ([], C.c_char_p),
     "mpf_status_string": ([_I], C.c_char_p),
     "mpf_gather": ([_I, _I, _I, _P, _L, _L, _P, _L, _P, _L, _P, _P, _P, _P, _I, _P, _P], _I),
     "mpf_scatter": ([_I, _I, _I, _P, _L, _P, _L, _L, _P, _L, _P, _P, _P, _P, _I, _P, _P], _I),
@@ -57,7 +58,7 @@ _SIGNATURES = {
     "mpf_add_density": ([_P, _P, _I, _P, C.c_int32, _L, _P, _P, _I, _P], _I),
     "mpf_num_tiles": ([_I, _I, _I, _P, _P, _P, _P], _I),
     "mpf_sort_workspace_bytes": ([_L, _L, _P], _I),
-    "mpf_sort_by_tile": ([_I, _I, _I, _P, _L, _P, _L, _L, _L, _P, _P, _P, _P, _P, _P, _P, _P, _P,
+    "mpf_sort_by_tile": ([_I, _I, _I, _P, _L, _P, _L, _L, _L, _P, _P, _P, _P, _P, _I, _P, _P, _P, _P,
                           C.c_size_t, _I, _P], _I),
     "mpf_permute_rows": ([_P, _L, _P, _L, _L, _P, _L, _I, _P], _I),
     "mpf_unpermute_rows": ([_P, _L, _P, _L, _L, _P, _L, _I, _P], _I),
@@ -99,7 +100,8 @@ def check(status: int, what: str) -> None:
     message = library().mpf_status_string(status).decode()
     if status in (ERR_ARGUMENT, ERR_SHAPE, ERR_ALIGNMENT, ERR_WORKSPACE, ERR_UNSUPPORTED):
         raise ValueError(f"{what}: {message} (status {status})")
-    raise BackendError(f"{what}: {message} (status {status})")
+    cuda = library().mpf_last_error().decode()
+    raise BackendError(f"{what}: {message} (status {status}, last CUDA error {cuda})")
 
 
 def require_cuda(*tensors: torch.Tensor) -> torch.device:

@@ -17,6 +17,16 @@ static std::atomic<long long> g_launches{0};
 
 void count_launches(int k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
 
+static std::atomic<int> g_last_error{0};
+
+int record_cuda_error(cudaError_t e) {
+    if (e == cudaSuccess) return MPF_OK;
+    g_last_error.store((int)e, std::memory_order_relaxed);
+    return MPF_ERR_CUDA;
+}
+
+int launch_status() { return record_cuda_error(cudaGetLastError()); }
+
 int sm_count() {
     int device = 0;
     if (cudaGetDevice(&device) != cudaSuccess) return 148;
@@ -63,6 +73,7 @@ static Grid<T> make_grid(int ndim, int degree, const double* lower, const double
         const bool on = d < ndim;
         g.lower[d] = on ? (T)lower[d] : T(0);
         g.cell[d] = on ? (T)cell[d] : T(1);
+        g.inv[d] = T(1) / g.cell[d];  // host IEEE division in T: RN(1 / cell)
         g.num[d] = on ? num[d] : 1;
         g.code[d] = on ? code[d] : PERIODIC;
         g.ext[d] = on ? axis_extent(num[d], code[d], degree) : 1;
@@ -120,6 +131,11 @@ extern "C" {
 int mpf_version(void) { return 10000; }
 
 int64_t mpf_launch_count(void) { return (int64_t)g_launches.load(std::memory_order_relaxed); }
+
+const char* mpf_last_error(void) {
+    const int e = g_last_error.load(std::memory_order_relaxed);
+    return e == 0 ? "none" : cudaGetErrorName((cudaError_t)e);
+}
 
 const char* mpf_status_string(int status) {
     switch (status) {
@@ -347,19 +363,25 @@ int mpf_sort_workspace_bytes(int64_t n, int64_t num_tiles, size_t* bytes) {
 
 int mpf_sort_by_tile(int kind, int degree, int ndim, const void* positions, int64_t pos_stride, const void* values,
                      int64_t val_stride, int64_t ncomp, int64_t n, const double* lower, const double* cell,
-                     const int32_t* num, const int32_t* code, const int32_t* tile, uint32_t* keys, int32_t* order,
-                     int64_t* tile_start, void* workspace, size_t workspace_bytes, int dtype, void* stream) {
+                     const int32_t* num, const int32_t* code, const int32_t* tile, int within, uint32_t* keys,
+                     int32_t* order, int64_t* tile_start, void* workspace, size_t workspace_bytes, int dtype,
+                     void* stream) {
     if (!valid_kind(kind, degree) || (dtype != MPF_F64 && dtype != MPF_F32)) return MPF_ERR_ARGUMENT;
     MPF_TRY(check_grid(kind, degree, ndim, lower, cell, num, code));
     if (n < 0 || n > INT32_MAX) return MPF_ERR_ARGUMENT;
     int64_t ntiles = 0;
     MPF_TRY(mpf_num_tiles(kind, degree, ndim, num, code, tile, &ntiles));
+    if (within != 0 && within != 1) return MPF_ERR_ARGUMENT;
+    int64_t cells = 1;
+    if (within)
+        for (int d = 0; d < ndim; ++d) cells *= tile[d];
+    if ((uint64_t)ntiles * (uint64_t)cells >= ((uint64_t)1 << 32)) return MPF_ERR_ARGUMENT;
     MPF_TRY(check_rows(positions, pos_stride, n, ndim, dtype));
     if (values) {
         if (ncomp < 1) return MPF_ERR_ARGUMENT;
         MPF_TRY(check_rows(values, val_stride, n, (int)ncomp, dtype));
     }
-    if (!keys || !order || !tile_start) return MPF_ERR_ARGUMENT;
+    if (!tile_start || (n > 0 && (!keys || !order))) return MPF_ERR_ARGUMENT;
     if (workspace_bytes < sort_workspace_bytes(n) || (!workspace && n > 0)) return MPF_ERR_WORKSPACE;
     if ((reinterpret_cast<uintptr_t>(workspace) % 256) != 0) return MPF_ERR_ALIGNMENT;
     const cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -375,7 +397,7 @@ int mpf_sort_by_tile(int kind, int degree, int ndim, const void* positions, int6
                 a.tile[d] = d < ndim ? tile[d] : 1;
                 a.ntiles[d] = d < ndim ? (a.g.ext[d] + a.tile[d] - 1) / a.tile[d] : 1;
             }
-            a.sentinel = (uint32_t)ntiles; a.keys = keys;
+            a.sentinel = (uint32_t)(ntiles * cells); a.within = within; a.keys = keys;
             st = tile_keys<double>(kind, degree, ndim, a, s);
         } else {
             KeyArgs<float> a;
@@ -387,12 +409,12 @@ int mpf_sort_by_tile(int kind, int degree, int ndim, const void* positions, int6
                 a.tile[d] = d < ndim ? tile[d] : 1;
                 a.ntiles[d] = d < ndim ? (a.g.ext[d] + a.tile[d] - 1) / a.tile[d] : 1;
             }
-            a.sentinel = (uint32_t)ntiles; a.keys = keys;
+            a.sentinel = (uint32_t)(ntiles * cells); a.within = within; a.keys = keys;
             st = tile_keys<float>(kind, degree, ndim, a, s);
         }
         if (st != MPF_OK) return st;
     }
-    return sort_keys(keys, n, ntiles, order, tile_start, workspace, s);
+    return sort_keys(keys, n, ntiles, cells, order, tile_start, workspace, s);
 }
 
 int mpf_permute_rows(void* dst, int64_t dst_stride, const void* src, int64_t src_stride, int64_t rows,

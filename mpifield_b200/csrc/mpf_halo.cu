@@ -111,7 +111,7 @@ static int run_halo(T* f, int ndim, const int32_t* stored, int64_t ncomp, int h,
         if (fold) halo_fold_kernel<T><<<(unsigned)blocks, block, 0, stream>>>(f, v, periodic[axis]);
         else halo_fill_kernel<T><<<(unsigned)blocks, block, 0, stream>>>(f, v);
         count_launches(1);
-        if (cudaGetLastError() != cudaSuccess) return MPF_ERR_CUDA;
+        if (launch_status() != MPF_OK) return MPF_ERR_CUDA;
     }
     return MPF_OK;
 }
@@ -129,7 +129,7 @@ static int run_density(T* dst, const T* dep, int ndim, const int32_t* num, int h
         (T)(ndim > 1 ? cell[1] : 1.0), (T)(ndim > 2 ? cell[2] : 1.0), periodic[0],
         ndim > 1 ? periodic[1] : 1, ndim > 2 ? periodic[2] : 1);
     count_launches(1);
-    return cudaGetLastError() == cudaSuccess ? MPF_OK : MPF_ERR_CUDA;
+    return launch_status();
 }
 
 int halo_fill(void* f, int ndim, const int32_t* stored, int64_t ncomp, int h, const int32_t* periodic,

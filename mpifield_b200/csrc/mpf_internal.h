@@ -12,6 +12,7 @@ namespace mpf {
 template <typename T> struct Grid {
     T lower[3];
     T cell[3];
+    T inv[3];  // RN(1 / cell), for the correctly rounded (x - lower) / cell
     int num[3];
     int code[3];
     int ext[3];
@@ -42,6 +43,8 @@ struct Tuning {
     int ctas_per_sm; // resident CTAs per SM the grid is sized for
 };
 
+template <typename T, int NDIM>
+int node_launch(int op, int kind, int degree, const NodeArgs<T>& a, const Tuning& t, cudaStream_t stream);
 template <typename T>
 int launch_gather(int kind, int degree, int ndim, const NodeArgs<T>& a, const Tuning& t,
                   cudaStream_t stream);
@@ -79,6 +82,7 @@ template <typename T> struct KeyArgs {
     int64_t n;
     int tile[3];
     int64_t ntiles[3];
+    int within;  // 1: the key continues with the cell inside the tile
     uint32_t sentinel;
     uint32_t* keys;
 };
@@ -98,8 +102,8 @@ int add_density(void* dst, const void* dep, int ndim, const int32_t* num, int h,
 template <typename T>
 int tile_keys(int kind, int degree, int ndim, const KeyArgs<T>& a, cudaStream_t stream);
 size_t sort_workspace_bytes(int64_t n);
-int sort_keys(const uint32_t* keys, int64_t n, int64_t num_tiles, int32_t* order, int64_t* tile_start,
-              void* workspace, cudaStream_t stream);
+int sort_keys(const uint32_t* keys, int64_t n, int64_t num_tiles, int64_t cells, int32_t* order,
+              int64_t* tile_start, void* workspace, cudaStream_t stream);
 int permute_rows(void* dst, int64_t ds, const void* src, int64_t ss, int64_t rows, const int32_t* order,
                  int64_t n, int dtype, cudaStream_t stream);
 
@@ -110,5 +114,9 @@ int sm_count();
 
 // Counts kernel launches of this library (read by mpf_launch_count).
 void count_launches(int k);
+
+// MPF_OK after a launch, or MPF_ERR_CUDA with the CUDA error recorded for mpf_last_error.
+int launch_status();
+int record_cuda_error(cudaError_t e);
 
 }  // namespace mpf

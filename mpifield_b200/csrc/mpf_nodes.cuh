@@ -33,7 +33,7 @@ constexpr int kMaxBlock = 256;
 
 template <typename T>
 __device__ __forceinline__ T rel_of(const NodeArgs<T>& a, int d, int64_t i) {
-    return (a.pos[d * a.pos_stride + i] - a.g.lower[d]) / a.g.cell[d];
+    return div_rn(a.pos[d * a.pos_stride + i] - a.g.lower[d], a.g.cell[d], a.g.inv[d]);
 }
 
 // Block-wide min of lo[] and max of hi[] over NDIM axes, into s_lo / s_hi (which the
@@ -126,7 +126,7 @@ __device__ __forceinline__ void stencil_sum(const T* __restrict__ src, const I (
 // dst[(off) * ncomp + c0 + c] += W * v[c] with atomic adds.
 template <typename T, int NDIM, int S, int NCC, typename I>
 __device__ __forceinline__ void stencil_add(T* dst, const I (&off)[3][S], const T (&w)[3][S],
-                                            I ncomp, int c0, const T* v) {
+                                            I ncomp, int c0, const T (&v)[NCC]) {
     constexpr int SY = NDIM > 1 ? S : 1;
     constexpr int SZ = NDIM > 2 ? S : 1;
 #pragma unroll
@@ -145,24 +145,135 @@ __device__ __forceinline__ void stencil_add(T* dst, const I (&off)[3][S], const 
     }
 }
 
-// The pre-mapping node j of a box entry k (node-major, ncomp innermost) and its
-// component: k = ((jx * ey + jy) * ez + jz) * ncomp + c.
+// A box of the grid in shared memory: pre-mapping node lo[d] .. lo[d] + ex[d] - 1 per
+// axis, node-major with the components innermost.
+struct Box {
+    int lo[3];
+    int ex[3];
+};
+
+// The rows of a box: every row runs along the last axis, ex[NDIM-1] * ncomp elements,
+// contiguous in shared memory and (away from a periodic seam) in global memory. One warp
+// per row; the row's node prefix is mapped once, the last axis per element (with no
+// mapping when the row lies inside the grid). Int32 arithmetic throughout: a box holds
+// at most the shared memory of a CTA.
 template <int NDIM>
-__device__ __forceinline__ int64_t box_to_global(int64_t k, int ncomp, const int* lo, const int* ex,
-                                                 const int* num, const int* code, const int* ext,
-                                                 int* comp) {
-    *comp = (int)(k % ncomp);
-    int64_t node = k / ncomp;
-    int j[3] = {0, 0, 0};
+__device__ __forceinline__ int box_rows(const Box& b) {
+    int rows = 1;
 #pragma unroll
-    for (int d = NDIM - 1; d >= 0; --d) {
-        j[d] = (int)(node % ex[d]);
-        node /= ex[d];
+    for (int d = 0; d < NDIM - 1; ++d) rows *= b.ex[d];
+    return rows;
+}
+
+template <int NDIM, typename G>
+__device__ __forceinline__ int64_t row_prefix(int r, const Box& b, const G& g) {
+    // global node index of (row r, last-axis node 0), before the last axis is added
+    int64_t prefix = 0;
+    if constexpr (NDIM == 3) {
+        const int jx = r / b.ex[1];
+        const int jy = r - jx * b.ex[1];
+        prefix = ((int64_t)map_node(b.lo[0] + jx, g.num[0], g.code[0]) * g.ext[1] +
+                  map_node(b.lo[1] + jy, g.num[1], g.code[1])) * g.ext[2];
+    } else if constexpr (NDIM == 2) {
+        prefix = (int64_t)map_node(b.lo[0] + r, g.num[0], g.code[0]) * g.ext[1];
     }
-    int64_t g = 0;
+    return prefix;
+}
+
+// tile <- the box of the field (a gather's staging).
+template <typename T, int NDIM, int NC>
+__device__ __forceinline__ void stage_box(T* __restrict__ tile, const T* __restrict__ field, const Box& b,
+                                          const Grid<T>& g, int ncomp_rt) {
+    const int ncomp = NC > 0 ? NC : ncomp_rt;
+    constexpr int L = NDIM - 1;
+    const int last = b.ex[L];
+    const int rowlen = last * ncomp;
+    const int rows = box_rows<NDIM>(b);
+    const int lane = threadIdx.x & 31;
+    const int nwarps = blockDim.x >> 5;
+    const bool inside = g.code[L] == CLAMPED || (b.lo[L] >= 0 && b.lo[L] + last <= g.num[L]);
+    for (int r = threadIdx.x >> 5; r < rows; r += nwarps) {
+        const int64_t prefix = row_prefix<NDIM>(r, b, g);
+        T* dst = tile + r * rowlen;
+        if (inside) {
+            const T* src = field + (prefix + b.lo[L]) * ncomp;
+            for (int e = lane; e < rowlen; e += 32) dst[e] = __ldg(src + e);
+        } else {
+            for (int e = lane; e < rowlen; e += 32) {
+                const int j = e / ncomp;
+                const int c = e - j * ncomp;
+                dst[e] = __ldg(field + (prefix + map_node(b.lo[L] + j, g.num[L], g.code[L])) * ncomp + c);
+            }
+        }
+    }
+}
+
+// field += the non-zero entries of the box (a scatter's flush), global atomics.
+template <typename T, int NDIM, int NC>
+__device__ __forceinline__ void flush_box(const T* __restrict__ tile, T* field, const Box& b, const Grid<T>& g,
+                                          int ncomp_rt) {
+    const int ncomp = NC > 0 ? NC : ncomp_rt;
+    constexpr int L = NDIM - 1;
+    const int last = b.ex[L];
+    const int rowlen = last * ncomp;
+    const int rows = box_rows<NDIM>(b);
+    const int lane = threadIdx.x & 31;
+    const int nwarps = blockDim.x >> 5;
+    for (int r = threadIdx.x >> 5; r < rows; r += nwarps) {
+        const int64_t prefix = row_prefix<NDIM>(r, b, g);
+        const T* src = tile + r * rowlen;
+        for (int e = lane; e < rowlen; e += 32) {
+            const T v = src[e];
+            if (v != T(0)) {
+                const int j = e / ncomp;
+                const int c = e - j * ncomp;
+                atomicAdd(field + (prefix + map_node(b.lo[L] + j, g.num[L], g.code[L])) * ncomp + c, v);
+            }
+        }
+    }
+}
+
+template <int NDIM>
+__device__ __forceinline__ bool box_holds(const Box& b, const int* lo, const int* hi_last) {
 #pragma unroll
-    for (int d = 0; d < NDIM; ++d) g = g * ext[d] + map_node(lo[d] + j[d], num[d], code[d]);
-    return g;
+    for (int d = 0; d < NDIM; ++d)
+        if (lo[d] < b.lo[d] || hi_last[d] > b.lo[d] + b.ex[d] - 1) return false;
+    return true;
+}
+
+// The box for a chunk whose stencils span pre-mapping nodes lo[d] .. hi[d] + S - 1: the
+// span widened by the largest margin (2, 1 or 0 nodes a side) that still fits
+// `capacity` elements, so that the next chunks of the same cell tile fall inside it.
+// On a clamped-knot axis (no mapping) the box stays inside the array. Returns false
+// when not even the bare span fits.
+template <int NDIM, int S, typename G>
+__device__ __forceinline__ bool choose_box(const int* lo, const int* hi, int ncomp, int capacity, const G& g,
+                                           Box& b) {
+    for (int margin = 2; margin >= 0; --margin) {
+        int64_t vol = ncomp;
+#pragma unroll
+        for (int d = 0; d < NDIM; ++d) {
+            int first = lo[d] - margin;
+            int end = hi[d] + S + margin;  // one past the last node
+            if (g.code[d] == CLAMPED) {
+                first = max(first, 0);
+                end = min(end, g.ext[d]);
+            }
+            b.lo[d] = first;
+            b.ex[d] = end - first;
+            vol *= b.ex[d];
+        }
+        if (vol <= (int64_t)capacity) return true;
+    }
+    return false;
+}
+
+// The chunks of CTA `block`: a contiguous range, so that consecutive chunks of a CTA
+// come from the same cell tile when the markers are sorted by tile.
+__device__ __forceinline__ void chunk_range(int64_t nchunks, int64_t& first, int64_t& last) {
+    const int64_t per = (nchunks + gridDim.x - 1) / gridDim.x;
+    first = (int64_t)blockIdx.x * per;
+    last = min(first + per, nchunks);
 }
 
 template <typename T, int NDIM, int KIND, int P, int NC>
@@ -175,7 +286,11 @@ __global__ void __launch_bounds__(kMaxBlock) gather_kernel(const NodeArgs<T> a) 
     const int ncomp = NC > 0 ? NC : a.ncomp;
     const int64_t chunk = (int64_t)MPT * blockDim.x;
     const int64_t nchunks = (a.n + chunk - 1) / chunk;
-    for (int64_t ci = blockIdx.x; ci < nchunks; ci += gridDim.x) {
+    int64_t c_first, c_last;
+    chunk_range(nchunks, c_first, c_last);
+    Box box;
+    bool have_box = false;
+    for (int64_t ci = c_first; ci < c_last; ++ci) {
         const int64_t first = ci * chunk;
         T rel[MPT][NDIM];
         int lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
@@ -194,7 +309,6 @@ __global__ void __launch_bounds__(kMaxBlock) gather_kernel(const NodeArgs<T> a) 
             }
         }
         bool staged = false;
-        int blo[3] = {0, 0, 0}, bex[3] = {1, 1, 1};
         if (!a.force_global) {
             if (threadIdx.x < 3) {
                 s_lo[threadIdx.x] = INT_MAX;
@@ -203,22 +317,24 @@ __global__ void __launch_bounds__(kMaxBlock) gather_kernel(const NodeArgs<T> a) 
             __syncthreads();
             block_box<NDIM>(lo, hi, s_lo, s_hi);
             __syncthreads();
-            int64_t vol = 1;
+            int clo[3], chi[3], top[3];
 #pragma unroll
             for (int d = 0; d < NDIM; ++d) {
-                blo[d] = s_lo[d];
-                bex[d] = s_hi[d] - s_lo[d] + S;
-                vol *= bex[d];
+                clo[d] = s_lo[d];
+                chi[d] = s_hi[d];
+                top[d] = chi[d] + S - 1;
             }
-            staged = vol * ncomp <= (int64_t)a.capacity;
-            if (staged) {
-                const int64_t total = vol * ncomp;
-                for (int64_t k = threadIdx.x; k < total; k += blockDim.x) {
-                    int c;
-                    const int64_t g = box_to_global<NDIM>(k, ncomp, blo, bex, a.g.num, a.g.code, a.g.ext, &c);
-                    tile[k] = __ldg(a.field_in + g * ncomp + c);
+            if (have_box && box_holds<NDIM>(box, clo, top)) {
+                staged = true;
+            } else {
+                Box nb;
+                if (choose_box<NDIM, S>(clo, chi, ncomp, a.capacity, a.g, nb)) {
+                    stage_box<T, NDIM, NC>(tile, a.field_in, nb, a.g, ncomp);
+                    box = nb;
+                    have_box = true;
+                    staged = true;
+                    __syncthreads();
                 }
-                __syncthreads();
             }
         }
 #pragma unroll
@@ -238,7 +354,7 @@ __global__ void __launch_bounds__(kMaxBlock) gather_kernel(const NodeArgs<T> a) 
             }
             if (staged) {
                 int off[3][S];
-                box_offsets<NDIM, S, int>(base, blo, bex, off);
+                box_offsets<NDIM, S, int>(base, box.lo, box.ex, off);
                 if constexpr (NC > 0) {
                     T acc[NCC];
                     stencil_sum<T, NDIM, S, NCC, false, int>(tile, off, w, NC, 0, acc);
@@ -268,7 +384,8 @@ __global__ void __launch_bounds__(kMaxBlock) gather_kernel(const NodeArgs<T> a) 
                 }
             }
         }
-        __syncthreads();
+        // the box may be restaged by the next chunk only when every thread is done with it
+        if (!a.force_global) __syncthreads();
     }
 }
 
@@ -282,7 +399,11 @@ __global__ void __launch_bounds__(kMaxBlock) scatter_kernel(const NodeArgs<T> a)
     const int ncomp = NC > 0 ? NC : a.ncomp;
     const int64_t chunk = (int64_t)MPT * blockDim.x;
     const int64_t nchunks = (a.n + chunk - 1) / chunk;
-    for (int64_t ci = blockIdx.x; ci < nchunks; ci += gridDim.x) {
+    int64_t c_first, c_last;
+    chunk_range(nchunks, c_first, c_last);
+    Box box;
+    bool have_box = false;  // the box holds deposits not yet flushed
+    for (int64_t ci = c_first; ci < c_last; ++ci) {
         const int64_t first = ci * chunk;
         T rel[MPT][NDIM];
         T val[MPT][NCC];
@@ -317,9 +438,6 @@ __global__ void __launch_bounds__(kMaxBlock) scatter_kernel(const NodeArgs<T> a)
             }
         }
         bool staged = false;
-        bool empty = false;
-        int blo[3] = {0, 0, 0}, bex[3] = {1, 1, 1};
-        int64_t total = 0;
         if (!a.force_global) {
             if (threadIdx.x < 3) {
                 s_lo[threadIdx.x] = INT_MAX;
@@ -328,23 +446,32 @@ __global__ void __launch_bounds__(kMaxBlock) scatter_kernel(const NodeArgs<T> a)
             __syncthreads();
             block_box<NDIM>(lo, hi, s_lo, s_hi);
             __syncthreads();
-            int64_t vol = 1;
+            int clo[3], chi[3], top[3];
+            bool empty = false;
 #pragma unroll
             for (int d = 0; d < NDIM; ++d) {
-                if (s_hi[d] < s_lo[d]) empty = true;
-                blo[d] = s_lo[d];
-                bex[d] = s_hi[d] - s_lo[d] + S;
-                vol *= bex[d];
+                clo[d] = s_lo[d];
+                chi[d] = s_hi[d];
+                top[d] = chi[d] + S - 1;
+                if (chi[d] < clo[d]) empty = true;
             }
-            if (empty) {
-                __syncthreads();
-                continue;
-            }
-            total = vol * ncomp;
-            staged = total <= (int64_t)a.capacity;
-            if (staged) {
-                for (int64_t k = threadIdx.x; k < total; k += blockDim.x) tile[k] = T(0);
-                __syncthreads();
+            if (empty) continue;  // no live marker in the chunk (uniform across the CTA)
+            if (have_box && box_holds<NDIM>(box, clo, top)) {
+                staged = true;
+            } else {
+                Box nb;
+                if (choose_box<NDIM, S>(clo, chi, ncomp, a.capacity, a.g, nb)) {
+                    if (have_box) flush_box<T, NDIM, NC>(tile, a.field_out, box, a.g, ncomp);
+                    __syncthreads();
+                    int total = ncomp;
+#pragma unroll
+                    for (int d = 0; d < NDIM; ++d) total *= nb.ex[d];
+                    for (int k = threadIdx.x; k < total; k += blockDim.x) tile[k] = T(0);
+                    __syncthreads();
+                    box = nb;
+                    have_box = true;
+                    staged = true;
+                }
             }
         }
         T* dst = staged ? tile : a.field_out;
@@ -365,13 +492,13 @@ __global__ void __launch_bounds__(kMaxBlock) scatter_kernel(const NodeArgs<T> a)
             }
             if (staged) {
                 int off[3][S];
-                box_offsets<NDIM, S, int>(base, blo, bex, off);
+                box_offsets<NDIM, S, int>(base, box.lo, box.ex, off);
                 if constexpr (NC > 0) {
                     stencil_add<T, NDIM, S, NCC, int>(dst, off, w, NC, 0, val[m]);
                 } else {
                     for (int c = 0; c < ncomp; ++c) {
-                        const T v = a.values[c * a.val_stride + i];
-                        stencil_add<T, NDIM, S, 1, int>(dst, off, w, ncomp, c, &v);
+                        const T v[1] = {a.values[c * a.val_stride + i]};
+                        stencil_add<T, NDIM, S, 1, int>(dst, off, w, ncomp, c, v);
                     }
                 }
             } else {
@@ -381,24 +508,17 @@ __global__ void __launch_bounds__(kMaxBlock) scatter_kernel(const NodeArgs<T> a)
                     stencil_add<T, NDIM, S, NCC, int64_t>(dst, off, w, NC, 0, val[m]);
                 } else {
                     for (int c = 0; c < ncomp; ++c) {
-                        const T v = a.values[c * a.val_stride + i];
-                        stencil_add<T, NDIM, S, 1, int64_t>(dst, off, w, ncomp, c, &v);
+                        const T v[1] = {a.values[c * a.val_stride + i]};
+                        stencil_add<T, NDIM, S, 1, int64_t>(dst, off, w, ncomp, c, v);
                     }
                 }
             }
         }
-        if (staged) {
-            __syncthreads();
-            for (int64_t k = threadIdx.x; k < total; k += blockDim.x) {
-                const T v = tile[k];
-                if (v != T(0)) {
-                    int c;
-                    const int64_t g = box_to_global<NDIM>(k, ncomp, blo, bex, a.g.num, a.g.code, a.g.ext, &c);
-                    atomicAdd(a.field_out + g * ncomp + c, v);
-                }
-            }
-        }
+        if (!a.force_global) __syncthreads();
+    }
+    if (have_box) {
         __syncthreads();
+        flush_box<T, NDIM, NC>(tile, a.field_out, box, a.g, ncomp);
     }
 }
 

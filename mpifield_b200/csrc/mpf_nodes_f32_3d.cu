@@ -1,0 +1,6 @@
+// mpf_nodes_f32_3d.cu -- the 3D node kernels instantiated for float.
+#include "mpf_nodes_launch.cuh"
+
+namespace mpf {
+template int node_launch<float, 3>(int, int, int, const NodeArgs<float>&, const Tuning&, cudaStream_t);
+}  // namespace mpf

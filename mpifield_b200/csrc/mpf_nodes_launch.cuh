@@ -8,11 +8,17 @@
 
 namespace mpf {
 
-// The dynamic shared memory a kernel may take above the 48 KB default, set once per
-// kernel and device.
-template <typename K> static cudaError_t allow_smem(K kernel, int bytes) {
-    if (bytes <= 48 * 1024) return cudaSuccess;
-    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+// Lets a kernel take `bytes` of dynamic shared memory (its static shared memory comes on
+// top, so even 48 KB needs the attribute). Set once per kernel instantiation, device and
+// size: `cache` is the instantiation's own table of the largest size set per device.
+template <typename K> static int allow_smem(K kernel, int bytes, int* cache) {
+    if (bytes <= 0) return MPF_OK;
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= 64) device = 0;
+    if (cache[device] >= bytes) return MPF_OK;
+    const int st = record_cuda_error(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    if (st == MPF_OK) cache[device] = bytes;
+    return st;
 }
 
 struct LaunchShape {
@@ -43,10 +49,11 @@ static int run_gather(NodeArgs<T> a, const Tuning& t, cudaStream_t stream) {
     a.force_global = staged_path ? 0 : 1;
     a.capacity = s.smem / (int)sizeof(T);
     auto kernel = gather_kernel<T, NDIM, KIND, P, NC>;
-    if (allow_smem(kernel, s.smem) != cudaSuccess) return MPF_ERR_CUDA;
+    static int cache[64] = {0};
+    if (allow_smem(kernel, s.smem, cache) != MPF_OK) return MPF_ERR_CUDA;
     kernel<<<s.grid, s.block, s.smem, stream>>>(a);
     count_launches(1);
-    return cudaGetLastError() == cudaSuccess ? MPF_OK : MPF_ERR_CUDA;
+    return launch_status();
 }
 
 template <typename T, int NDIM, int KIND, int P, int NC>
@@ -56,10 +63,11 @@ static int run_scatter(NodeArgs<T> a, const Tuning& t, cudaStream_t stream) {
     a.force_global = staged_path ? 0 : 1;
     a.capacity = s.smem / (int)sizeof(T);
     auto kernel = scatter_kernel<T, NDIM, KIND, P, NC>;
-    if (allow_smem(kernel, s.smem) != cudaSuccess) return MPF_ERR_CUDA;
+    static int cache[64] = {0};
+    if (allow_smem(kernel, s.smem, cache) != MPF_OK) return MPF_ERR_CUDA;
     kernel<<<s.grid, s.block, s.smem, stream>>>(a);
     count_launches(1);
-    return cudaGetLastError() == cudaSuccess ? MPF_OK : MPF_ERR_CUDA;
+    return launch_status();
 }
 
 template <typename T, int NDIM, int KIND, int P>
@@ -68,7 +76,7 @@ static int run_gather_grad(const NodeArgs<T>& a, cudaStream_t stream) {
     const int64_t blocks = std::min<int64_t>((a.n + block - 1) / block, (int64_t)sm_count() * 8);
     gather_grad_kernel<T, NDIM, KIND, P><<<(unsigned)std::max<int64_t>(blocks, 1), block, 0, stream>>>(a);
     count_launches(1);
-    return cudaGetLastError() == cudaSuccess ? MPF_OK : MPF_ERR_CUDA;
+    return launch_status();
 }
 
 // The component count as a template argument for 1-3 components, a run-time loop above.
@@ -125,26 +133,13 @@ static int grad_by_kind(int kind, int degree, const NodeArgs<T>& a, cudaStream_t
     return MPF_ERR_ARGUMENT;
 }
 
-template <typename T>
-int launch_gather(int kind, int degree, int ndim, const NodeArgs<T>& a, const Tuning& t,
-                  cudaStream_t stream) {
-    return by_dimension<T, false>(kind, degree, ndim, a, t, stream);
-}
-
-template <typename T>
-int launch_scatter(int kind, int degree, int ndim, const NodeArgs<T>& a, const Tuning& t,
-                   cudaStream_t stream) {
-    return by_dimension<T, true>(kind, degree, ndim, a, t, stream);
-}
-
-template <typename T>
-int launch_gather_grad(int kind, int degree, int ndim, const NodeArgs<T>& a, cudaStream_t stream) {
-    switch (ndim) {
-        case 1: return grad_by_kind<T, 1>(kind, degree, a, stream);
-        case 2: return grad_by_kind<T, 2>(kind, degree, a, stream);
-        case 3: return grad_by_kind<T, 3>(kind, degree, a, stream);
-    }
-    return MPF_ERR_ARGUMENT;
+// One dimension's node launches (op 0 gather, 1 scatter, 2 position gradient); each
+// element type and dimension is instantiated in a translation unit of its own.
+template <typename T, int NDIM>
+int node_launch(int op, int kind, int degree, const NodeArgs<T>& a, const Tuning& t, cudaStream_t stream) {
+    if (op == 0) return by_kind<T, NDIM, false>(kind, degree, a, t, stream);
+    if (op == 1) return by_kind<T, NDIM, true>(kind, degree, a, t, stream);
+    return grad_by_kind<T, NDIM>(kind, degree, a, stream);
 }
 
 }  // namespace mpf

@@ -12,7 +12,7 @@ static int run_deposit(const PathArgs<T>& a, cudaStream_t stream) {
     const int64_t blocks = std::min<int64_t>((a.n + block - 1) / block, (int64_t)sm_count() * 16);
     deposit_paths_kernel<T, NDIM, P, WHITNEY><<<(unsigned)std::max<int64_t>(blocks, 1), block, 0, stream>>>(a);
     count_launches(1);
-    return cudaGetLastError() == cudaSuccess ? MPF_OK : MPF_ERR_CUDA;
+    return launch_status();
 }
 
 template <typename T, int NDIM, int P, bool WHITNEY>
@@ -21,7 +21,7 @@ static int run_gather_edges(const PathArgs<T>& a, cudaStream_t stream) {
     const int64_t blocks = std::min<int64_t>((a.n + block - 1) / block, (int64_t)sm_count() * 16);
     gather_edges_kernel<T, NDIM, P, WHITNEY><<<(unsigned)std::max<int64_t>(blocks, 1), block, 0, stream>>>(a);
     count_launches(1);
-    return cudaGetLastError() == cudaSuccess ? MPF_OK : MPF_ERR_CUDA;
+    return launch_status();
 }
 
 template <typename T, int NDIM, bool GATHER>

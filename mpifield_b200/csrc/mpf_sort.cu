@@ -21,7 +21,6 @@ namespace mpf {
 constexpr int kSortBlock = 256;
 constexpr int kSortItems = 16;  // keys per thread per tile
 constexpr int kSortTile = kSortBlock * kSortItems;
-constexpr int kDigits = 256;
 constexpr int kWarps = kSortBlock / 32;
 
 
@@ -37,29 +36,39 @@ __global__ void tile_keys_kernel(const KeyArgs<T> a) {
                 continue;
             }
         }
-        int64_t key = 0;
+        int64_t key = 0, inner = 0;
 #pragma unroll
         for (int d = 0; d < NDIM; ++d) {
-            const T rel = (a.pos[d * a.pos_stride + i] - a.g.lower[d]) / a.g.cell[d];
+            const T rel = div_rn(a.pos[d * a.pos_stride + i] - a.g.lower[d], a.g.cell[d], a.g.inv[d]);
             const int anchor = axis_anchor<T, KIND, P>(rel, a.g.num[d], a.g.code[d]);
-            key = key * a.ntiles[d] + anchor / a.tile[d];
+            const int t = anchor / a.tile[d];
+            key = key * a.ntiles[d] + t;
+            inner = inner * a.tile[d] + (anchor - t * a.tile[d]);
+        }
+        if (a.within) {
+            int64_t cells = 1;
+#pragma unroll
+            for (int d = 0; d < NDIM; ++d) cells *= a.tile[d];
+            key = key * cells + inner;
         }
         a.keys[i] = (uint32_t)key;
     }
 }
 
+template <int BITS>
 __global__ void digit_histogram_kernel(const uint32_t* keys, int64_t n, int shift, uint32_t* counts,
                                        int64_t nblocks) {
-    __shared__ uint32_t hist[kDigits];
-    for (int d = threadIdx.x; d < kDigits; d += blockDim.x) hist[d] = 0;
+    constexpr int DIGITS = 1 << BITS;
+    __shared__ uint32_t hist[DIGITS];
+    for (int d = threadIdx.x; d < DIGITS; d += blockDim.x) hist[d] = 0;
     __syncthreads();
     const int64_t base = (int64_t)blockIdx.x * kSortTile;
     for (int k = threadIdx.x; k < kSortTile; k += blockDim.x) {
         const int64_t i = base + k;
-        if (i < n) atomicAdd(&hist[(keys[i] >> shift) & 0xff], 1u);
+        if (i < n) atomicAdd(&hist[(keys[i] >> shift) & (DIGITS - 1)], 1u);
     }
     __syncthreads();
-    for (int d = threadIdx.x; d < kDigits; d += blockDim.x) counts[(int64_t)d * nblocks + blockIdx.x] = hist[d];
+    for (int d = threadIdx.x; d < DIGITS; d += blockDim.x) counts[(int64_t)d * nblocks + blockIdx.x] = hist[d];
 }
 
 // Exclusive scan of `count` u32 values in place, in three kernels: chunk sums, a scan of
@@ -134,16 +143,19 @@ __global__ void scan_chunks_kernel(uint32_t* data, int64_t count, const uint32_t
 
 // The stable scatter of one pass. Warp w of a CTA owns the contiguous segment
 // [w * 32 * kSortItems, (w + 1) * 32 * kSortItems) of the CTA's tile and walks it in
-// rounds of 32 consecutive keys.
+// rounds of 32 consecutive keys; the per-warp digit counts live in dynamic shared
+// memory (kWarps << BITS words) and become the warps' output offsets in place.
+template <int BITS>
 __global__ void digit_scatter_kernel(const uint32_t* keys_in, const int32_t* vals_in, int64_t n,
                                      int shift, const uint32_t* offsets, int64_t nblocks,
                                      uint32_t* keys_out, int32_t* vals_out) {
-    __shared__ uint32_t warp_count[kWarps][kDigits];
-    __shared__ uint32_t warp_base[kWarps][kDigits];
+    constexpr int DIGITS = 1 << BITS;
+    extern __shared__ uint32_t warp_count[];  // [kWarps][DIGITS]
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    for (int d = threadIdx.x; d < kWarps * kDigits; d += blockDim.x) (&warp_count[0][0])[d] = 0;
+    for (int d = threadIdx.x; d < kWarps * DIGITS; d += blockDim.x) warp_count[d] = 0;
     __syncthreads();
+    uint32_t* mine = warp_count + warp * DIGITS;
     const int64_t seg = (int64_t)blockIdx.x * kSortTile + (int64_t)warp * 32 * kSortItems;
     uint32_t key[kSortItems];
     int32_t val[kSortItems];
@@ -155,23 +167,24 @@ __global__ void digit_scatter_kernel(const uint32_t* keys_in, const int32_t* val
         const bool have = i < n;
         key[r] = have ? keys_in[i] : 0xffffffffu;
         val[r] = have ? (vals_in ? vals_in[i] : (int32_t)i) : 0;
-        const uint32_t digit = (key[r] >> shift) & 0xff;
+        const uint32_t digit = (key[r] >> shift) & (DIGITS - 1);
         // lanes holding the same digit this round, and those of them before this lane
         const unsigned same = __match_any_sync(0xffffffffu, have ? (int)digit : -1 - lane);
         const unsigned before = __popc(same & below);
-        const uint32_t count = have ? warp_count[warp][digit] : 0;
+        const uint32_t count = have ? mine[digit] : 0;
         rank[r] = count + before;
         __syncwarp();
-        if (have && before == 0) warp_count[warp][digit] = count + __popc(same);
+        if (have && before == 0) mine[digit] = count + __popc(same);
         __syncwarp();
     }
     __syncthreads();
-    // the offset of every warp's digit run inside the CTA, then in the whole array
-    for (int d = threadIdx.x; d < kDigits; d += blockDim.x) {
+    // every warp's run of a digit starts after the CTA's earlier warps, in the whole array
+    for (int d = threadIdx.x; d < DIGITS; d += blockDim.x) {
         uint32_t s = offsets[(int64_t)d * nblocks + blockIdx.x];
         for (int w = 0; w < kWarps; ++w) {
-            warp_base[w][d] = s;
-            s += warp_count[w][d];
+            const uint32_t c = warp_count[w * DIGITS + d];
+            warp_count[w * DIGITS + d] = s;
+            s += c;
         }
     }
     __syncthreads();
@@ -179,20 +192,22 @@ __global__ void digit_scatter_kernel(const uint32_t* keys_in, const int32_t* val
     for (int r = 0; r < kSortItems; ++r) {
         const int64_t i = seg + (int64_t)r * 32 + lane;
         if (i < n) {
-            const uint32_t digit = (key[r] >> shift) & 0xff;
-            const uint32_t dst = warp_base[warp][digit] + rank[r];
+            const uint32_t digit = (key[r] >> shift) & (DIGITS - 1);
+            const uint32_t dst = mine[digit] + rank[r];
             keys_out[dst] = key[r];
             vals_out[dst] = val[r];
         }
     }
 }
 
-// tile_start[k] = the first rank whose key is >= k, k = 0 .. num_tiles; tile_start[num_tiles + 1] = n.
-__global__ void tile_starts_kernel(const uint32_t* sorted, int64_t n, int64_t num_tiles, int64_t* start) {
+// tile_start[t] = the first rank whose tile is >= t, t = 0 .. num_tiles (the sentinel tile
+// of dead markers); tile_start[num_tiles + 1] = n. A key's tile is key / cells.
+__global__ void tile_starts_kernel(const uint32_t* sorted, int64_t n, int64_t num_tiles, int64_t cells,
+                                   int64_t* start) {
     for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j <= n;
          j += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t prev = j == 0 ? -1 : (int64_t)sorted[j - 1];
-        const int64_t cur = j == n ? num_tiles + 1 : (int64_t)sorted[j];
+        const int64_t prev = j == 0 ? -1 : (int64_t)sorted[j - 1] / cells;
+        const int64_t cur = j == n ? num_tiles + 1 : (int64_t)sorted[j] / cells;
         for (int64_t k = prev + 1; k <= cur && k <= num_tiles + 1; ++k) start[k] = (k == num_tiles + 1) ? n : j;
     }
 }
@@ -233,7 +248,7 @@ struct SortLayout {
 static SortLayout sort_layout(int64_t n) {
     SortLayout L;
     const int64_t nb = sort_blocks(n);
-    const int64_t count = nb * kDigits;
+    const int64_t count = nb * (1 << 10);
     size_t off = 0;
     L.keys_a = off; off += align256(sizeof(uint32_t) * std::max<int64_t>(n, 1));
     L.keys_b = off; off += align256(sizeof(uint32_t) * std::max<int64_t>(n, 1));
@@ -255,7 +270,7 @@ static int scan_exclusive(uint32_t* data, int64_t count, uint32_t* sums, cudaStr
     count_launches(1);
     scan_chunks_kernel<<<(unsigned)chunks, kSortBlock, 0, stream>>>(data, count, sums);
     count_launches(1);
-    return cudaGetLastError() == cudaSuccess ? MPF_OK : MPF_ERR_CUDA;
+    return launch_status();
 }
 
 template <typename T, int NDIM, int KIND, int P>
@@ -264,7 +279,7 @@ static int run_keys(const KeyArgs<T>& a, cudaStream_t stream) {
     const int64_t blocks = std::min<int64_t>((a.n + block - 1) / block, (int64_t)sm_count() * 16);
     tile_keys_kernel<T, NDIM, KIND, P><<<(unsigned)std::max<int64_t>(blocks, 1), block, 0, stream>>>(a);
     count_launches(1);
-    return cudaGetLastError() == cudaSuccess ? MPF_OK : MPF_ERR_CUDA;
+    return launch_status();
 }
 
 template <typename T, int NDIM>
@@ -290,14 +305,36 @@ int tile_keys(int kind, int degree, int ndim, const KeyArgs<T>& a, cudaStream_t 
     return MPF_ERR_ARGUMENT;
 }
 
+template <int BITS>
+static int radix_pass(const uint32_t* kin, const int32_t* vin, int64_t n, int shift, uint32_t* counts,
+                      uint32_t* sums, int64_t nb, uint32_t* kout, int32_t* vout, cudaStream_t stream) {
+    digit_histogram_kernel<BITS><<<(unsigned)nb, kSortBlock, 0, stream>>>(kin, n, shift, counts, nb);
+    count_launches(1);
+    if (launch_status() != MPF_OK) return MPF_ERR_CUDA;
+    const int st = scan_exclusive(counts, nb << BITS, sums, stream);
+    if (st != MPF_OK) return st;
+    const int smem = kWarps * (1 << BITS) * (int)sizeof(uint32_t);
+    static int configured = 0;
+    if (configured < smem) {
+        if (record_cuda_error(cudaFuncSetAttribute(digit_scatter_kernel<BITS>,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != MPF_OK)
+            return MPF_ERR_CUDA;
+        configured = smem;
+    }
+    digit_scatter_kernel<BITS><<<(unsigned)nb, kSortBlock, smem, stream>>>(kin, vin, n, shift, counts, nb, kout, vout);
+    count_launches(1);
+    return launch_status();
+}
+
 // Sort (keys, marker) pairs stably; the marker order lands in `order`, the tile starts
-// in `tile_start`.
-int sort_keys(const uint32_t* keys, int64_t n, int64_t num_tiles, int32_t* order, int64_t* tile_start,
-              void* workspace, cudaStream_t stream) {
+// in `tile_start`. Keys are below max_key + 1 (max_key, the sentinel, included); the
+// passes take 8 to 10 bits each, as few passes as 10-bit digits allow.
+int sort_keys(const uint32_t* keys, int64_t n, int64_t num_tiles, int64_t cells, int32_t* order,
+              int64_t* tile_start, void* workspace, cudaStream_t stream) {
     if (n == 0) {
-        tile_starts_kernel<<<1, 256, 0, stream>>>(nullptr, 0, num_tiles, tile_start);
+        tile_starts_kernel<<<1, 256, 0, stream>>>(nullptr, 0, num_tiles, cells, tile_start);
         count_launches(1);
-        return cudaGetLastError() == cudaSuccess ? MPF_OK : MPF_ERR_CUDA;
+        return launch_status();
     }
     const SortLayout L = sort_layout(n);
     char* ws = static_cast<char*>(workspace);
@@ -307,9 +344,11 @@ int sort_keys(const uint32_t* keys, int64_t n, int64_t num_tiles, int32_t* order
     int32_t* vb = reinterpret_cast<int32_t*>(ws + L.vals_b);
     uint32_t* counts = reinterpret_cast<uint32_t*>(ws + L.counts);
     uint32_t* sums = reinterpret_cast<uint32_t*>(ws + L.sums);
+    const uint64_t max_key = (uint64_t)num_tiles * (uint64_t)cells;  // the sentinel
     int bits = 1;
-    while (bits < 32 && ((uint64_t)num_tiles >> bits) != 0) ++bits;  // the sentinel num_tiles included
-    const int passes = std::max(1, (bits + 7) / 8);
+    while (bits < 32 && (max_key >> bits) != 0) ++bits;
+    const int passes = std::max(1, (bits + 9) / 10);
+    const int digit_bits = std::max(8, (bits + passes - 1) / passes);
     const int64_t nb = sort_blocks(n);
     const uint32_t* kin = keys;
     const int32_t* vin = nullptr;  // the first pass numbers the markers itself
@@ -317,25 +356,22 @@ int sort_keys(const uint32_t* keys, int64_t n, int64_t num_tiles, int32_t* order
     int32_t* vout_buf[2] = {va, vb};
     uint32_t* kout = ka;
     for (int p = 0; p < passes; ++p) {
-        const int shift = 8 * p;
+        const int shift = digit_bits * p;
         kout = kout_buf[p & 1];
         int32_t* vout = (p == passes - 1) ? order : vout_buf[p & 1];
-        digit_histogram_kernel<<<(unsigned)nb, kSortBlock, 0, stream>>>(kin, n, shift, counts, nb);
-        count_launches(1);
-        if (cudaGetLastError() != cudaSuccess) return MPF_ERR_CUDA;
-        int st = scan_exclusive(counts, nb * kDigits, sums, stream);
+        int st;
+        if (digit_bits <= 8) st = radix_pass<8>(kin, vin, n, shift, counts, sums, nb, kout, vout, stream);
+        else if (digit_bits == 9) st = radix_pass<9>(kin, vin, n, shift, counts, sums, nb, kout, vout, stream);
+        else st = radix_pass<10>(kin, vin, n, shift, counts, sums, nb, kout, vout, stream);
         if (st != MPF_OK) return st;
-        digit_scatter_kernel<<<(unsigned)nb, kSortBlock, 0, stream>>>(kin, vin, n, shift, counts, nb, kout, vout);
-        count_launches(1);
-        if (cudaGetLastError() != cudaSuccess) return MPF_ERR_CUDA;
         kin = kout;
         vin = vout;
     }
     const int block = 256;
     const int64_t blocks = std::min<int64_t>((n + 1 + block - 1) / block, (int64_t)sm_count() * 16);
-    tile_starts_kernel<<<(unsigned)std::max<int64_t>(blocks, 1), block, 0, stream>>>(kout, n, num_tiles, tile_start);
+    tile_starts_kernel<<<(unsigned)std::max<int64_t>(blocks, 1), block, 0, stream>>>(kout, n, num_tiles, cells, tile_start);
     count_launches(1);
-    return cudaGetLastError() == cudaSuccess ? MPF_OK : MPF_ERR_CUDA;
+    return launch_status();
 }
 
 int permute_rows(void* dst, int64_t ds, const void* src, int64_t ss, int64_t rows, const int32_t* order,
@@ -349,7 +385,7 @@ int permute_rows(void* dst, int64_t ds, const void* src, int64_t ss, int64_t row
         permute_rows_kernel<float><<<(unsigned)std::max<int64_t>(blocks, 1), block, 0, stream>>>(
             (float*)dst, ds, (const float*)src, ss, rows, order, n);
     count_launches(1);
-    return cudaGetLastError() == cudaSuccess ? MPF_OK : MPF_ERR_CUDA;
+    return launch_status();
 }
 
 int unpermute_rows(void* dst, int64_t ds, const void* src, int64_t ss, int64_t rows, const int32_t* order,
@@ -363,7 +399,7 @@ int unpermute_rows(void* dst, int64_t ds, const void* src, int64_t ss, int64_t r
         unpermute_rows_kernel<float><<<(unsigned)std::max<int64_t>(blocks, 1), block, 0, stream>>>(
             (float*)dst, ds, (const float*)src, ss, rows, order, n);
     count_launches(1);
-    return cudaGetLastError() == cudaSuccess ? MPF_OK : MPF_ERR_CUDA;
+    return launch_status();
 }
 
 template int tile_keys<double>(int, int, int, const KeyArgs<double>&, cudaStream_t);

@@ -40,6 +40,19 @@ __host__ __device__ __forceinline__ int axis_extent(int num, int code, int degre
     return code == CLAMPED ? num + degree - 1 : num;
 }
 
+// a / b, correctly rounded, from rb = RN(1 / b): q0 = RN(a rb), one Newton step with the
+// exact residual a - q b (an FMA) makes q1 faithful, and Markstein's correction
+// q = RN(q1 + (a - q1 b) rb) is then the correctly rounded quotient (P. Markstein,
+// "Computation of elementary functions on the IBM RISC System/6000 processor", IBM J.
+// Res. Dev. 34 (1990); Handbook of Floating-Point Arithmetic, ch. 5). Non-finite results
+// (infinite or NaN operands, overflow) take the IEEE division.
+template <typename T> __device__ __forceinline__ T div_rn(T a, T b, T rb) {
+    const T q0 = a * rb;
+    const T q1 = fma(fma(-q0, b, a), rb, q0);
+    const T q = fma(fma(-q1, b, a), rb, q1);
+    return isfinite(q) ? q : a / b;
+}
+
 // rel - num * floor(rel / num): the periodic wrap of the reference stencils.
 template <typename T> __device__ __forceinline__ T wrap_period(T rel, int num) {
     const T n = (T)num;
@@ -135,7 +148,8 @@ __device__ __forceinline__ int axis_stencil(T rel, int num, int code, T* w) {
     if constexpr (KIND == LINEAR) {
         int left;
         if (code == PERIODIC) {
-            rel = wrap_period(rel, num);
+            // for 0 < rel < num - 1 the quotient rel / num rounds below 1: the wrap is exact identity
+            if (!(rel > T(0) && rel < T(num - 1))) rel = wrap_period(rel, num);
             left = trunc_int<T>(rel) % num;
             if (left < 0) left += num;
         } else {
@@ -151,7 +165,7 @@ __device__ __forceinline__ int axis_stencil(T rel, int num, int code, T* w) {
     } else if constexpr (KIND == QUADRATIC) {
         int c;
         if (code == PERIODIC) {
-            rel = wrap_period(rel, num);
+            if (!(rel > T(0) && rel < T(num - 1))) rel = wrap_period(rel, num);
             c = clampi(trunc_int<T>(rel + T(0.5)), 0, num);
         } else {
             if (rel < T(0)) rel = T(0);

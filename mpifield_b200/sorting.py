@@ -5,7 +5,8 @@ kernels need (each chunk of markers then touches one small box of the grid). The
 a marker is the tile of its stencil's anchor node (the node LINEAR, QUADRATIC or the
 spline stencil is anchored on), row-major over tiles of ``tile`` nodes per axis; a
 marker whose values are all zero goes to the sentinel tile ``num_tiles`` without its
-position being read. The order is stable: equal keys keep the marker order, so the
+position being read (with ``within`` the key continues with the cell inside the tile).
+The order is stable: equal keys keep the marker order, so the
 result equals ``numpy.argsort(keys, kind="stable")`` bit for bit. The workspace is
 allocated here by torch and passed to the C call, which allocates nothing.
 """
@@ -48,8 +49,14 @@ def num_tiles(weighting, geometry, tile) -> int:
     return int(out.value)
 
 
-def sort_by_tile(positions: torch.Tensor, weighting, geometry, tile, values: torch.Tensor | None = None) -> TileOrder:
-    """Sort markers by cell tile (see the module docstring)."""
+def sort_by_tile(positions: torch.Tensor, weighting, geometry, tile, values: torch.Tensor | None = None,
+                 within: bool = False) -> TileOrder:
+    """Sort markers by cell tile (see the module docstring).
+
+    With ``within`` the key continues with the anchor cell inside the tile, so markers of
+    one cell end up next to each other (tile-major, then cell-major): the order the
+    gather and scatter kernels run fastest on.
+    """
     kind, degree = _kind_of(weighting)
     lower, cell, num, code, ndim = _lib.geometry_arrays(geometry)
     device = _lib.require_cuda(positions)
@@ -70,7 +77,7 @@ def sort_by_tile(positions: torch.Tensor, weighting, geometry, tile, values: tor
     else:
         vptr, vs, ncomp = None, 0, 0
     status = _lib.library().mpf_sort_by_tile(
-        kind, degree, ndim, pos.data_ptr(), ps, vptr, vs, ncomp, n, lower, cell, num, code, t,
+        kind, degree, ndim, pos.data_ptr(), ps, vptr, vs, ncomp, n, lower, cell, num, code, t, int(bool(within)),
         keys.data_ptr(), order.data_ptr(), tile_start.data_ptr(), workspace.data_ptr(), workspace.numel(),
         _lib.dtype_code(dtype), _lib.stream_of(device))
     _lib.check(status, "sort_by_tile")

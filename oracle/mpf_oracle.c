@@ -794,9 +794,12 @@ void og_gather_edges(int ndim, int degree, const double* pos, int64_t pos_stride
 void og_tile_keys(int kind, int degree, int ndim, const double* pos, int64_t pos_stride,
                   const double* values, int64_t val_stride, int64_t ncomp, int64_t n,
                   const double* lower, const double* cell, const int32_t* num,
-                  const int32_t* code, const int32_t* tile, uint32_t* keys) {
+                  const int32_t* code, const int32_t* tile, int within, uint32_t* keys) {
     int64_t ntiles[3] = {1, 1, 1};
     int64_t total = 1;
+    int64_t cells = 1;
+    if (within)
+        for (int d = 0; d < ndim; ++d) cells *= tile[d];
     for (int d = 0; d < ndim; ++d) {
         const int e = og_extent(num[d], code[d], degree);
         ntiles[d] = (e + tile[d] - 1) / tile[d];
@@ -808,11 +811,11 @@ void og_tile_keys(int kind, int degree, int ndim, const double* pos, int64_t pos
             for (int64_t c = 0; c < ncomp; ++c)
                 if (values[c * val_stride + i] != 0.0) live = 1;
             if (!live) {
-                keys[i] = (uint32_t)total;
+                keys[i] = (uint32_t)(total * cells);
                 continue;
             }
         }
-        int64_t key = 0;
+        int64_t key = 0, inner = 0;
         for (int d = 0; d < ndim; ++d) {
             og_axis s;
             const double rel = (pos[d * pos_stride + i] - lower[d]) / cell[d];
@@ -823,7 +826,9 @@ void og_tile_keys(int kind, int degree, int ndim, const double* pos, int64_t pos
             else if (code[d] == 2) anchor = s.node[0];
             else anchor = s.node[degree / 2];
             key = key * ntiles[d] + anchor / tile[d];
+            inner = inner * tile[d] + anchor % tile[d];
         }
+        if (within) key = key * cells + inner;
         keys[i] = (uint32_t)key;
     }
 }

@@ -57,7 +57,7 @@ def _declare(lib: C.CDLL) -> None:
         "og_deposit_whitney": [_I, _P, _L, _P, _L, _P, _L, _P, _P, _P, _P, _P],
         "og_deposit_spline": [_I, _I, _P, _L, _P, _L, _P, _L, _P, _P, _P, _P, _P],
         "og_gather_edges": [_I, _I, _P, _L, _L, _P, _P, _L, _P, _P, _P, _P],
-        "og_tile_keys": [_I, _I, _I, _P, _L, _P, _L, _L, _L, _P, _P, _P, _P, _P, _P],
+        "og_tile_keys": [_I, _I, _I, _P, _L, _P, _L, _L, _L, _P, _P, _P, _P, _P, _I, _P],
         "cb_gather": [_I, _I, _I, _P, _L, _L, _P, _L, _P, _L, _P, _P, _P, _P, _I],
         "cb_scatter": [_I, _I, _I, _P, _L, _P, _L, _L, _P, _L, _P, _P, _P, _P, _I],
         "cb_deposit_whitney": [_I, _P, _L, _P, _L, _P, _L, _P, _P, _P, _P, _P, _I],
@@ -185,7 +185,7 @@ def gather_edges(degree: int, positions, edges, geometry) -> np.ndarray:
     return result
 
 
-def tile_keys(kind, degree: int, positions, geometry, tile, values=None) -> np.ndarray:
+def tile_keys(kind, degree: int, positions, geometry, tile, values=None, within: bool = False) -> np.ndarray:
     """The cell-tile key of every marker (uint32); dead markers get the sentinel key."""
     lower, cell, num, code = split_geometry(geometry)
     pos, ps = _rows(positions)
@@ -198,7 +198,7 @@ def tile_keys(kind, degree: int, positions, geometry, tile, values=None) -> np.n
         vals, vs = _rows(values)
         vptr, ncomp = _ptr(vals), vals.shape[0]
     library().og_tile_keys(_kind(kind), degree, lower.size, _ptr(pos), ps, vptr, vs, ncomp, n,
-                           _ptr(lower), _ptr(cell), _ptr(num), _ptr(code), _ptr(tile),
+                           _ptr(lower), _ptr(cell), _ptr(num), _ptr(code), _ptr(tile), int(bool(within)),
                            _ptr(keys))
     return keys
 

@@ -89,12 +89,14 @@ def test_tile_keys_and_order_are_bit_exact(kind, degree, ndim):
         values[:, ::5] = 0.0
         pos[:, ::10] = np.nan  # dead markers: keys without reading the position
         tile = (8, 4, 2)[:ndim]
-        t = mf.sort_by_tile(cu(pos), (KIND_NAMES[kind], degree), geom, tile, cu(values))
-        keys = O.tile_keys(kind, degree, pos, geom, tile, values)
-        np.testing.assert_array_equal(t.keys.cpu().numpy().view(np.uint32), keys)
-        np.testing.assert_array_equal(t.order.cpu().numpy(), O.sort_by_tile(keys))
-        starts = np.searchsorted(np.sort(keys), np.arange(t.num_tiles + 1), side="left")
-        np.testing.assert_array_equal(t.tile_start.cpu().numpy(), np.append(starts, keys.size))
+        for within in (False, True):
+            t = mf.sort_by_tile(cu(pos), (KIND_NAMES[kind], degree), geom, tile, cu(values), within=within)
+            keys = O.tile_keys(kind, degree, pos, geom, tile, values, within=within)
+            np.testing.assert_array_equal(t.keys.cpu().numpy().view(np.uint32), keys)
+            np.testing.assert_array_equal(t.order.cpu().numpy(), O.sort_by_tile(keys))
+            cells = int(np.prod(tile)) if within else 1
+            starts = np.searchsorted(np.sort(keys) // cells, np.arange(t.num_tiles + 1), side="left")
+            np.testing.assert_array_equal(t.tile_start.cpu().numpy(), np.append(starts, keys.size))
 
 
 def test_sort_edge_cases_and_permute():
@@ -108,10 +110,29 @@ def test_sort_edge_cases_and_permute():
     pos = np.random.default_rng(0).uniform(0, 1, (3, 1000))
     order = torch.randperm(1000, device=DEV).to(torch.int32)
     np.testing.assert_array_equal(mf.permute(cu(pos), order).cpu().numpy(), pos[:, order.cpu().numpy()])
+    # a 25-bit key (256^3 cells within 8^3 tiles) takes three passes
+    pos = np.random.default_rng(1).uniform(0, 1, (3, 200_000))
+    geom3 = (0.0, 0.0, 0.0, 1 / 256, 1 / 256, 1 / 256, 256, 256, 256, 1, 1, 1)
+    t = mf.sort_by_tile(cu(pos), (1, 2), geom3, (8, 8, 8), within=True)
+    keys = O.tile_keys("quadratic", 2, pos, geom3, (8, 8, 8), within=True)
+    np.testing.assert_array_equal(t.order.cpu().numpy(), O.sort_by_tile(keys))
     # equal keys keep the marker order (the sort is stable) for many equal keys
     same = np.full((1, 100_000), 0.55)
     t = mf.sort_by_tile(cu(same), (1, 2), geom, (3,))
     np.testing.assert_array_equal(t.order.cpu().numpy(), np.arange(100_000))
+
+
+def test_correctly_rounded_division_matches_the_gpu_division():
+    """The reciprocal-based quotient the kernels use for (x - lower) / h is bit-identical to
+    the IEEE division: checked through the cell keys of markers near cell boundaries."""
+    rng = np.random.default_rng(12)
+    for h in (1 / 256, 0.1, 0.3, 1 / 3, 7.0, 1e-3, 2.0 ** -20 * 3):
+        k = rng.integers(0, 200, 100_000)
+        x = (k * h) * (1 + rng.integers(-4, 5, k.size) * 2.0 ** -52)
+        geom = (0.0, h, 200, 1)
+        t = mf.sort_by_tile(cu(x[None]), (0, 1), geom, (1,))
+        np.testing.assert_array_equal(t.keys.cpu().numpy().view(np.uint32),
+                                      O.tile_keys("linear", 1, x[None], geom, (1,)))
 
 
 @pytest.mark.parametrize("kind,degree", [("linear", 1), ("quadratic", 2), ("spline", 1), ("spline", 2), ("spline", 3)])

@@ -295,6 +295,9 @@ def test_tile_keys_and_stable_order():
     for k in np.unique(keys):
         idx = order[keys[order] == k]
         assert (np.diff(idx) > 0).all()  # stable
+    inner = O.tile_keys("quadratic", 2, pos, geom, (4, 4, 4), values, within=True)
+    assert inner.max() == 27 * 64
+    np.testing.assert_array_equal(inner[keys < 27] // 64, keys[keys < 27])
 
 
 def test_adjoint_identity_of_the_oracle():
