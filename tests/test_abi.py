@@ -82,7 +82,7 @@ def test_invalid_arguments_return_a_status_before_any_device_work():
     assert lib.mpf_halo_fold(fake, 1, stored, 1, 2, per, 0, None) == _lib.ERR_SHAPE
     # a workspace too small
     t = (C.c_int32 * 3)(4, 4, 4)
-    assert lib.mpf_sort_by_tile(1, 2, 3, fake, 0, None, 0, 0, 1000, lower, cell, num, code, t, fake, fake, fake,
+    assert lib.mpf_sort_by_tile(1, 2, 3, fake, 0, None, 0, 0, 1000, lower, cell, num, code, t, 0, fake, fake, fake,
                                 fake, 16, 0, None) == _lib.ERR_WORKSPACE
 
 
