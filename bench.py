@@ -60,6 +60,7 @@ def parse() -> argparse.Namespace:
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=("ours", "reference"), default="ours")
     p.add_argument("--markers", type=int, default=1 << 26)
+    p.add_argument("--grid", type=int, default=256, help="nodes per axis (smaller grids for profiling)")
     p.add_argument("--dtype", choices=("f64", "f32"), default="f64")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
@@ -504,7 +505,9 @@ def run_reference(args, world, rank) -> None:
 
 
 def main() -> None:
+    global GRID
     args = parse()
+    GRID = args.grid
     world, rank, local = dist_setup(args)
     try:
         if args.impl == "reference":

@@ -82,6 +82,14 @@ MPF_API int64_t mpf_launch_count(void);
 /* The name of the last CUDA error behind an MPF_ERR_CUDA status ("none" if there was none). */
 MPF_API const char* mpf_last_error(void);
 
+/*
+ * The error bits the kernels of the current device raised since the last clear
+ * (MPF_DEVICE_ERROR_WAIT: a bounded wait on a bulk copy gave up and the CTA left early,
+ * so results of that launch are incomplete). Synchronous; clears them when `clear`.
+ */
+#define MPF_DEVICE_ERROR_WAIT 1u
+MPF_API int mpf_device_errors(int clear, uint32_t* flags);
+
 /* A static, human-readable name of a status code. */
 MPF_API const char* mpf_status_string(int status);
 

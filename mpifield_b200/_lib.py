@@ -47,6 +47,7 @@ _SIGNATURES = {
     "mpf_version": ([], _I),
     "mpf_launch_count": ([], _L),
     "mpf_last_error": ([], C.c_char_p),
+    "mpf_device_errors": ([_I, _P], _I),
     "mpf_status_string": ([_I], C.c_char_p),
     "mpf_gather": ([_I, _I, _I, _P, _L, _L, _P, _L, _P, _L, _P, _P, _P, _P, _I, _P, _P], _I),
     "mpf_scatter": ([_I, _I, _I, _P, _L, _P, _L, _L, _P, _L, _P, _P, _P, _P, _I, _P, _P], _I),
@@ -150,3 +151,10 @@ def geometry_arrays(geometry) -> tuple[C.Array, C.Array, C.Array, C.Array, int]:
 
 def tuning_struct(path: int = PATH_AUTO, block: int = 0, smem_bytes: int = 0, ctas_per_sm: int = 0) -> Tuning:
     return Tuning(path, block, smem_bytes, ctas_per_sm)
+
+
+def device_errors(clear: bool = True) -> int:
+    """The MPF_DEVICE_ERROR_* bits raised by kernels on the current device (synchronises)."""
+    flags = C.c_uint32(0)
+    check(library().mpf_device_errors(int(clear), C.byref(flags)), "device_errors")
+    return int(flags.value)

@@ -27,6 +27,21 @@ int record_cuda_error(cudaError_t e) {
 
 int launch_status() { return record_cuda_error(cudaGetLastError()); }
 
+// Bits the kernels raise when a bounded wait gives up (one word per device).
+static __device__ unsigned g_device_errors;
+
+unsigned* device_error_word() {
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= 64) return nullptr;
+    static unsigned* words[64] = {nullptr};
+    if (!words[device]) {
+        void* p = nullptr;
+        if (record_cuda_error(cudaGetSymbolAddress(&p, g_device_errors)) != MPF_OK) return nullptr;
+        words[device] = static_cast<unsigned*>(p);
+    }
+    return words[device];
+}
+
 int sm_count() {
     int device = 0;
     if (cudaGetDevice(&device) != cudaSuccess) return 148;
@@ -131,6 +146,18 @@ extern "C" {
 int mpf_version(void) { return 10000; }
 
 int64_t mpf_launch_count(void) { return (int64_t)g_launches.load(std::memory_order_relaxed); }
+
+int mpf_device_errors(int clear, uint32_t* flags) {
+    if (!flags) return MPF_ERR_ARGUMENT;
+    unsigned value = 0;
+    if (record_cuda_error(cudaMemcpyFromSymbol(&value, g_device_errors, sizeof(value))) != MPF_OK) return MPF_ERR_CUDA;
+    *flags = value;
+    if (clear && value) {
+        const unsigned zero = 0;
+        if (record_cuda_error(cudaMemcpyToSymbol(g_device_errors, &zero, sizeof(zero))) != MPF_OK) return MPF_ERR_CUDA;
+    }
+    return MPF_OK;
+}
 
 const char* mpf_last_error(void) {
     const int e = g_last_error.load(std::memory_order_relaxed);

@@ -33,6 +33,8 @@ template <typename T> struct NodeArgs {
     int ncomp;
     int capacity;        // shared-memory box capacity, in elements of T
     int force_global;    // 1: never stage (the direct path), for tests and unsorted input
+    int bulk;            // 1: positions are 16-byte aligned rows, prefetched by bulk copies
+    unsigned* error;     // device word of MPF_DEVICE_ERROR_* bits
 };
 
 // The tuning of one launch (the autotuned table supplies it; zero fields take defaults).
@@ -114,6 +116,9 @@ int sm_count();
 
 // Counts kernel launches of this library (read by mpf_launch_count).
 void count_launches(int k);
+
+// The device word the kernels report MPF_DEVICE_ERROR_* bits in (per device), or NULL.
+unsigned* device_error_word();
 
 // MPF_OK after a launch, or MPF_ERR_CUDA with the CUDA error recorded for mpf_last_error.
 int launch_status();

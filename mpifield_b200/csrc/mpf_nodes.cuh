@@ -23,6 +23,7 @@
 
 #include "mpf_internal.h"
 #include "mpf_stencil.cuh"
+#include "mpifield_b200.h"
 
 namespace mpf {
 
@@ -276,35 +277,131 @@ __device__ __forceinline__ void chunk_range(int64_t nchunks, int64_t& first, int
     last = min(first + per, nchunks);
 }
 
+// ------------------------------------------------ bulk copies (TMA) and barriers --
+//
+// The gather prefetches the positions of its next chunk into shared memory with 1D bulk
+// copies (cp.async.bulk, no multicast) completing on an mbarrier; every wait is bounded
+// and a CTA that gives up records MPF_DEVICE_ERROR_WAIT in *a.error and leaves.
+
+constexpr int kWaitLimit = 1 << 22;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
+    for (int i = 0; i < kWaitLimit; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done) : "r"(smem_u32(bar)), "r"(parity) : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+// Puts the positions of chunk `ci` (count markers from `first`) into rows
+// buf[d * CH ...]: bulk copies of the 16-byte multiple, plain loads for the rest.
+// Called by one thread; the barrier completes when the bulk bytes have landed.
+template <typename T, int NDIM>
+__device__ __forceinline__ void issue_positions(const NodeArgs<T>& a, T* buf, int CH, int64_t first, int count,
+                                                uint64_t* bar) {
+    const unsigned bytes = (unsigned)count * (unsigned)sizeof(T);
+    const unsigned bulk = bytes & ~15u;
+    mbar_expect_tx(bar, bulk * NDIM);
+#pragma unroll
+    for (int d = 0; d < NDIM; ++d)
+        if (bulk) bulk_g2s(buf + d * CH, a.pos + d * a.pos_stride + first, bulk, bar);
+    for (int j = bulk / sizeof(T); j < count; ++j)
+#pragma unroll
+        for (int d = 0; d < NDIM; ++d) buf[d * CH + j] = a.pos[d * a.pos_stride + first + j];
+}
+
+template <typename T>
+__device__ __forceinline__ T rel_from(const T x, const Grid<T>& g, int d) {
+    return div_rn(x - g.lower[d], g.cell[d], g.inv[d]);
+}
+
+// The gather. Positions of chunk k wait in shared buffer k % 2 while the bulk copy of
+// chunk k + 1 fills the other; the field box is staged as described above.
 template <typename T, int NDIM, int KIND, int P, int NC>
-__global__ void __launch_bounds__(kMaxBlock) gather_kernel(const NodeArgs<T> a) {
+__global__ void __launch_bounds__(kMaxBlock, 2) gather_kernel(const NodeArgs<T> a) {
     constexpr int S = P + 1;
     constexpr int NCC = NC > 0 ? NC : 1;
     constexpr int MPT = kMarkersPerThread;
-    T* tile = reinterpret_cast<T*>(mpf_dynamic_smem);
+    __shared__ __align__(8) uint64_t bars[2];
     __shared__ int s_lo[3], s_hi[3];
     const int ncomp = NC > 0 ? NC : a.ncomp;
-    const int64_t chunk = (int64_t)MPT * blockDim.x;
-    const int64_t nchunks = (a.n + chunk - 1) / chunk;
+    const int CH = MPT * blockDim.x;
+    T* posbuf = reinterpret_cast<T*>(mpf_dynamic_smem);  // [2][NDIM][CH]
+    T* tile = posbuf + 2 * NDIM * CH;
+    const int64_t nchunks = (a.n + CH - 1) / CH;
     int64_t c_first, c_last;
     chunk_range(nchunks, c_first, c_last);
+    if (c_first >= c_last) return;
+    if (threadIdx.x == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        mbar_init_fence();
+    }
+    __syncthreads();
+    if (a.bulk && threadIdx.x == 0)
+        issue_positions<T, NDIM>(a, posbuf, CH, c_first * CH, (int)min((int64_t)CH, a.n - c_first * CH), &bars[0]);
     Box box;
     bool have_box = false;
     for (int64_t ci = c_first; ci < c_last; ++ci) {
-        const int64_t first = ci * chunk;
-        T rel[MPT][NDIM];
+        const int k = (int)(ci - c_first);
+        const int b = k & 1;
+        const int64_t first = ci * CH;
+        const int count = (int)min((int64_t)CH, a.n - first);
+        T* pb = posbuf + b * NDIM * CH;
+        if (a.bulk) {
+            if (threadIdx.x == 0 && ci + 1 < c_last) {
+                fence_proxy_async();
+                issue_positions<T, NDIM>(a, posbuf + (b ^ 1) * NDIM * CH, CH, first + CH,
+                                         (int)min((int64_t)CH, a.n - first - CH), &bars[b ^ 1]);
+            }
+            const bool late = !mbar_wait(&bars[b], (k >> 1) & 1);
+            if (__syncthreads_or(late)) {
+                if (threadIdx.x == 0) atomicOr(a.error, (unsigned)MPF_DEVICE_ERROR_WAIT);
+                // the copy that may still be in flight lands in this CTA's own buffer
+                if (threadIdx.x == 0 && ci + 1 < c_last) mbar_wait(&bars[b ^ 1], ((k + 1) >> 1) & 1);
+                __syncthreads();
+                return;
+            }
+        } else {
+            for (int j = threadIdx.x; j < count; j += blockDim.x)
+#pragma unroll
+                for (int d = 0; d < NDIM; ++d) pb[d * CH + j] = a.pos[d * a.pos_stride + first + j];
+            __syncthreads();
+        }
         int lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
 #pragma unroll
         for (int m = 0; m < MPT; ++m) {
-            const int64_t i = first + (int64_t)m * blockDim.x + threadIdx.x;
-            if (i < a.n) {
+            const int j = m * blockDim.x + threadIdx.x;
+            if (j < count) {
 #pragma unroll
                 for (int d = 0; d < NDIM; ++d) {
-                    rel[m][d] = rel_of(a, d, i);
                     T w[S];
-                    const int b = axis_stencil<T, KIND, P>(rel[m][d], a.g.num[d], a.g.code[d], w);
-                    lo[d] = min(lo[d], b);
-                    hi[d] = max(hi[d], b);
+                    const int base = axis_stencil<T, KIND, P>(rel_from(pb[d * CH + j], a.g, d), a.g.num[d],
+                                                              a.g.code[d], w);
+                    lo[d] = min(lo[d], base);
+                    hi[d] = max(hi[d], base);
                 }
             }
         }
@@ -339,14 +436,16 @@ __global__ void __launch_bounds__(kMaxBlock) gather_kernel(const NodeArgs<T> a) 
         }
 #pragma unroll
         for (int m = 0; m < MPT; ++m) {
-            const int64_t i = first + (int64_t)m * blockDim.x + threadIdx.x;
-            if (i >= a.n) continue;
+            const int j = m * blockDim.x + threadIdx.x;
+            if (j >= count) continue;
+            const int64_t i = first + j;
             T w[3][S];
             int base[3] = {0, 0, 0};
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
                 if (d < NDIM) {
-                    base[d] = axis_stencil<T, KIND, P>(rel[m][d], a.g.num[d], a.g.code[d], w[d]);
+                    base[d] = axis_stencil<T, KIND, P>(rel_from(pb[d * CH + j], a.g, d), a.g.num[d], a.g.code[d],
+                                                       w[d]);
                 } else {
 #pragma unroll
                     for (int s = 0; s < S; ++s) w[d][s] = T(s == 0);
@@ -384,34 +483,55 @@ __global__ void __launch_bounds__(kMaxBlock) gather_kernel(const NodeArgs<T> a) 
                 }
             }
         }
-        // the box may be restaged by the next chunk only when every thread is done with it
-        if (!a.force_global) __syncthreads();
+        // the positions buffer and the box are free once every thread is past this point
+        __syncthreads();
     }
 }
 
+template <int S, int NDIM> struct StencilPoints {
+    static constexpr int value = NDIM == 1 ? S : (NDIM == 2 ? S * S : S * S * S);
+};
+
+// The scatter. The markers of a chunk go to warps in contiguous runs of 32 (lane l of
+// warp w, step s: marker (w * MPT + s) * 32 + l of the chunk), so that in a marker store
+// sorted by cell the lanes of a warp hold markers of a few cells. For a box chunk, every
+// lane writes the stencil contributions of its marker into the warp's scratch
+// (a [stencil point][33] table); lane o then runs along the 32 markers summing
+// contribution o over runs of markers with the same stencil base, and adds each run's
+// sum to the box with one shared-memory add. Within an instruction the lanes add to
+// distinct nodes, so the adds of a warp never contend.
 template <typename T, int NDIM, int KIND, int P, int NC>
-__global__ void __launch_bounds__(kMaxBlock) scatter_kernel(const NodeArgs<T> a) {
+__global__ void __launch_bounds__(kMaxBlock, 2) scatter_kernel(const NodeArgs<T> a) {
     constexpr int S = P + 1;
     constexpr int NCC = NC > 0 ? NC : 1;
     constexpr int MPT = kMarkersPerThread;
-    T* tile = reinterpret_cast<T*>(mpf_dynamic_smem);
+    constexpr int SP = StencilPoints<S, NDIM>::value;
+    constexpr int ROWS = SP < 32 ? SP : 32;
+    constexpr int GROUPS = (SP + 31) / 32;
+    constexpr int PITCH = 33;
     __shared__ int s_lo[3], s_hi[3];
     const int ncomp = NC > 0 ? NC : a.ncomp;
-    const int64_t chunk = (int64_t)MPT * blockDim.x;
-    const int64_t nchunks = (a.n + chunk - 1) / chunk;
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int nwarps = blockDim.x >> 5;
+    const int CH = MPT * blockDim.x;
+    T* tile = reinterpret_cast<T*>(mpf_dynamic_smem);
+    T* scratch = tile + a.capacity + warp * (ROWS * PITCH);  // this warp's [ROWS][PITCH]
+    int* bidx = reinterpret_cast<int*>(tile + a.capacity + nwarps * (ROWS * PITCH)) + warp * 32;
+    const int64_t nchunks = (a.n + CH - 1) / CH;
     int64_t c_first, c_last;
     chunk_range(nchunks, c_first, c_last);
     Box box;
     bool have_box = false;  // the box holds deposits not yet flushed
     for (int64_t ci = c_first; ci < c_last; ++ci) {
-        const int64_t first = ci * chunk;
+        const int64_t first = ci * CH + (int64_t)warp * 32 * MPT;
         T rel[MPT][NDIM];
         T val[MPT][NCC];
         bool live[MPT];
         int lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
 #pragma unroll
         for (int m = 0; m < MPT; ++m) {
-            const int64_t i = first + (int64_t)m * blockDim.x + threadIdx.x;
+            const int64_t i = first + m * 32 + lane;
             live[m] = false;
             if (i < a.n) {
                 // a dead marker (all values zero) deposits nothing and its position,
@@ -474,42 +594,100 @@ __global__ void __launch_bounds__(kMaxBlock) scatter_kernel(const NodeArgs<T> a)
                 }
             }
         }
-        T* dst = staged ? tile : a.field_out;
+        if (staged) {
+            const int sy = NDIM > 2 ? box.ex[2] : 1;
+            const int sx = NDIM > 1 ? box.ex[1] * sy : 1;
 #pragma unroll
-        for (int m = 0; m < MPT; ++m) {
-            if (!live[m]) continue;
-            const int64_t i = first + (int64_t)m * blockDim.x + threadIdx.x;
-            T w[3][S];
-            int base[3] = {0, 0, 0};
+            for (int m = 0; m < MPT; ++m) {
+                // this lane's marker: its stencil base in the box (or -1) and weights
+                T w[3][S];
+                int bofs = -1;
+                if (live[m]) {
+                    int base[3] = {0, 0, 0};
 #pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                if (d < NDIM) {
-                    base[d] = axis_stencil<T, KIND, P>(rel[m][d], a.g.num[d], a.g.code[d], w[d]);
+                    for (int d = 0; d < NDIM; ++d)
+                        base[d] = axis_stencil<T, KIND, P>(rel[m][d], a.g.num[d], a.g.code[d], w[d]) - box.lo[d];
+                    bofs = base[0] * sx + (NDIM > 1 ? base[1] * sy : 0) + (NDIM > 2 ? base[2] : 0);
                 } else {
 #pragma unroll
-                    for (int s = 0; s < S; ++s) w[d][s] = T(s == 0);
+                    for (int d = 0; d < 3; ++d)
+#pragma unroll
+                        for (int s = 0; s < S; ++s) w[d][s] = T(0);
+                }
+                bidx[lane] = bofs;
+                // one component: the contributions, then the runs, group by group
+                auto deposit = [&](int c, T v) {
+#pragma unroll
+                    for (int g = 0; g < GROUPS; ++g) {
+                        // contributions of stencil points g * 32 + r, r < ROWS
+#pragma unroll
+                        for (int r = 0; r < ROWS; ++r) {
+                            const int o = g * 32 + r;
+                            if (o < SP) {
+                                const int ea = NDIM == 3 ? o / (S * S) : (NDIM == 2 ? o / S : o);
+                                const int eb = NDIM == 3 ? (o / S) % S : (NDIM == 2 ? o % S : 0);
+                                const int ee = NDIM == 3 ? o % S : 0;
+                                T wt = w[0][ea];
+                                if constexpr (NDIM > 1) wt = wt * w[1][eb];
+                                if constexpr (NDIM > 2) wt = wt * w[2][ee];
+                                scratch[r * PITCH + lane] = wt * v;
+                            }
+                        }
+                        __syncwarp();
+                        const int o = g * 32 + lane;
+                        if (lane < ROWS && o < SP) {
+                            const int ea = NDIM == 3 ? o / (S * S) : (NDIM == 2 ? o / S : o);
+                            const int eb = NDIM == 3 ? (o / S) % S : (NDIM == 2 ? o % S : 0);
+                            const int ee = NDIM == 3 ? o % S : 0;
+                            const int off = ea * sx + eb * sy + ee;
+                            T acc = T(0);
+                            int run = bidx[0];
+                            for (int j = 0; j < 32; ++j) {
+                                const int bj = bidx[j];
+                                if (bj != run) {
+                                    if (run >= 0) atomicAdd(tile + (run + off) * ncomp + c, acc);
+                                    acc = T(0);
+                                    run = bj;
+                                }
+                                acc += scratch[lane * PITCH + j];
+                            }
+                            if (run >= 0) atomicAdd(tile + (run + off) * ncomp + c, acc);
+                        }
+                        __syncwarp();
+                    }
+                };
+                if constexpr (NC > 0) {
+#pragma unroll
+                    for (int c = 0; c < NCC; ++c) deposit(c, live[m] ? val[m][c] : T(0));
+                } else {
+                    for (int c = 0; c < ncomp; ++c)
+                        deposit(c, live[m] ? a.values[c * a.val_stride + first + m * 32 + lane] : T(0));
                 }
             }
-            if (staged) {
-                int off[3][S];
-                box_offsets<NDIM, S, int>(base, box.lo, box.ex, off);
-                if constexpr (NC > 0) {
-                    stencil_add<T, NDIM, S, NCC, int>(dst, off, w, NC, 0, val[m]);
-                } else {
-                    for (int c = 0; c < ncomp; ++c) {
-                        const T v[1] = {a.values[c * a.val_stride + i]};
-                        stencil_add<T, NDIM, S, 1, int>(dst, off, w, ncomp, c, v);
+        } else {
+#pragma unroll
+            for (int m = 0; m < MPT; ++m) {
+                if (!live[m]) continue;
+                const int64_t i = first + m * 32 + lane;
+                T w[3][S];
+                int base[3] = {0, 0, 0};
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    if (d < NDIM) {
+                        base[d] = axis_stencil<T, KIND, P>(rel[m][d], a.g.num[d], a.g.code[d], w[d]);
+                    } else {
+#pragma unroll
+                        for (int s = 0; s < S; ++s) w[d][s] = T(s == 0);
                     }
                 }
-            } else {
                 int64_t off[3][S];
                 global_offsets<NDIM, S>(base, a.g.num, a.g.code, a.g.ext, off);
                 if constexpr (NC > 0) {
-                    stencil_add<T, NDIM, S, NCC, int64_t>(dst, off, w, NC, 0, val[m]);
+                    stencil_add<T, NDIM, S, NCC, int64_t>(a.field_out, off, w, NC, 0, val[m]);
                 } else {
                     for (int c = 0; c < ncomp; ++c) {
                         const T v[1] = {a.values[c * a.val_stride + i]};
-                        stencil_add<T, NDIM, S, 1, int64_t>(dst, off, w, ncomp, c, v);
+                        stencil_add<T, NDIM, S, 1, int64_t>(a.field_out, off, w, ncomp, c, v);
                     }
                 }
             }

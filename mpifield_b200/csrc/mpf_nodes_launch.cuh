@@ -21,51 +21,63 @@ template <typename K> static int allow_smem(K kernel, int bytes, int* cache) {
     return st;
 }
 
-struct LaunchShape {
-    int block;
-    int smem;
-    unsigned grid;
-};
+static int pick_block(const Tuning& t) {
+    int block = t.block > 0 ? std::min(t.block, kMaxBlock) : kMaxBlock;
+    return std::max(32, block / 32 * 32);
+}
 
-template <typename T>
-static LaunchShape node_shape(const NodeArgs<T>& a, const Tuning& t, bool staged_path) {
-    LaunchShape s;
-    s.block = t.block > 0 ? std::min(t.block, kMaxBlock) : kMaxBlock;
-    s.block = std::max(32, s.block / 32 * 32);
-    s.smem = staged_path ? (t.smem_bytes > 0 ? t.smem_bytes : 48 * 1024) : 0;
-    s.smem = std::min(s.smem, 227 * 1024);
-    const int64_t chunk = (int64_t)kMarkersPerThread * s.block;
-    const int64_t nchunks = (a.n + chunk - 1) / chunk;
-    const int per_sm = t.ctas_per_sm > 0 ? t.ctas_per_sm : (staged_path ? std::max(1, (200 * 1024) / std::max(s.smem, 1)) : 4);
-    const int64_t cap = (int64_t)sm_count() * std::min(per_sm, 2048 / s.block);
-    s.grid = (unsigned)std::max<int64_t>(1, std::min(nchunks, cap));
-    return s;
+static unsigned grid_for(int64_t nchunks, int smem, int block) {
+    // two CTAs per SM at most (the kernels are bounded to 128 registers for that)
+    const int by_smem = std::max(1, (227 * 1024) / std::max(smem, 1));
+    const int per_sm = std::min({2, by_smem, 2048 / block});
+    return (unsigned)std::max<int64_t>(1, std::min<int64_t>(nchunks, (int64_t)sm_count() * per_sm));
 }
 
 template <typename T, int NDIM, int KIND, int P, int NC>
 static int run_gather(NodeArgs<T> a, const Tuning& t, cudaStream_t stream) {
-    const bool staged_path = t.path != 1;
-    LaunchShape s = node_shape(a, t, staged_path);
-    a.force_global = staged_path ? 0 : 1;
-    a.capacity = s.smem / (int)sizeof(T);
+    const int block = pick_block(t);
+    const int CH = kMarkersPerThread * block;
+    const bool direct = t.path == 1;
+    const int pos_bytes = 2 * NDIM * CH * (int)sizeof(T);
+    int box_bytes = direct ? 0 : (t.smem_bytes > 0 ? t.smem_bytes : 48 * 1024);
+    box_bytes = std::min(box_bytes, 227 * 1024 - pos_bytes);
+    const int smem = pos_bytes + box_bytes;
+    a.force_global = direct ? 1 : 0;
+    a.capacity = box_bytes / (int)sizeof(T);
+    const uintptr_t p = reinterpret_cast<uintptr_t>(a.pos);
+    a.bulk = (p % 16 == 0) && (NDIM == 1 || (a.pos_stride * (int64_t)sizeof(T)) % 16 == 0) ? 1 : 0;
+    a.error = device_error_word();
+    if (!a.error) return MPF_ERR_CUDA;
     auto kernel = gather_kernel<T, NDIM, KIND, P, NC>;
     static int cache[64] = {0};
-    if (allow_smem(kernel, s.smem, cache) != MPF_OK) return MPF_ERR_CUDA;
-    kernel<<<s.grid, s.block, s.smem, stream>>>(a);
+    if (allow_smem(kernel, smem, cache) != MPF_OK) return MPF_ERR_CUDA;
+    const int64_t nchunks = (a.n + CH - 1) / CH;
+    kernel<<<grid_for(nchunks, smem, block), block, smem, stream>>>(a);
     count_launches(1);
     return launch_status();
 }
 
 template <typename T, int NDIM, int KIND, int P, int NC>
 static int run_scatter(NodeArgs<T> a, const Tuning& t, cudaStream_t stream) {
-    const bool staged_path = t.path != 1;
-    LaunchShape s = node_shape(a, t, staged_path);
-    a.force_global = staged_path ? 0 : 1;
-    a.capacity = s.smem / (int)sizeof(T);
+    constexpr int SP = StencilPoints<P + 1, NDIM>::value;
+    constexpr int ROWS = SP < 32 ? SP : 32;
+    const int block = pick_block(t);
+    const int CH = kMarkersPerThread * block;
+    const bool direct = t.path == 1;
+    int box_bytes = direct ? 0 : (t.smem_bytes > 0 ? t.smem_bytes : 40 * 1024);
+    const int scratch_bytes = direct ? 0 : (block / 32) * (ROWS * 33 * (int)sizeof(T) + 32 * (int)sizeof(int));
+    box_bytes = std::min(box_bytes, 227 * 1024 - scratch_bytes);
+    const int smem = box_bytes + scratch_bytes;
+    a.force_global = direct ? 1 : 0;
+    a.capacity = box_bytes / (int)sizeof(T);
+    a.bulk = 0;
+    a.error = device_error_word();
+    if (!a.error) return MPF_ERR_CUDA;
     auto kernel = scatter_kernel<T, NDIM, KIND, P, NC>;
     static int cache[64] = {0};
-    if (allow_smem(kernel, s.smem, cache) != MPF_OK) return MPF_ERR_CUDA;
-    kernel<<<s.grid, s.block, s.smem, stream>>>(a);
+    if (allow_smem(kernel, smem, cache) != MPF_OK) return MPF_ERR_CUDA;
+    const int64_t nchunks = (a.n + CH - 1) / CH;
+    kernel<<<grid_for(nchunks, smem, block), block, smem, stream>>>(a);
     count_launches(1);
     return launch_status();
 }

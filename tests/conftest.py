@@ -29,3 +29,16 @@ def pytest_collection_modifyitems(config, items):
     for item in items:
         if "gpu" in item.keywords:
             item.add_marker(skip)
+
+
+@pytest.fixture(autouse=True)
+def no_device_errors(request):
+    """GPU tests leave no bounded-wait error bits behind in the backend."""
+    yield
+    if "gpu" in request.keywords:
+        import torch
+
+        if torch.cuda.is_available():
+            from mpifield_b200 import _lib
+
+            assert _lib.device_errors(clear=True) == 0
