@@ -210,6 +210,26 @@ MPF_API int mpf_sort_by_tile(int kind, int degree, int ndim, const void* positio
                      int32_t* order, int64_t* tile_start, void* workspace, size_t workspace_bytes,
                      int dtype, void* stream);
 
+/*
+ * mpf_sort_by_tile without a workspace argument and without any allocation, for callers
+ * that cannot call cudaMalloc: work recorded into a CUDA graph (an allocation cannot be
+ * captured), a host application that owns all device memory through its own pool, or a
+ * real-time loop that cannot take the implicit synchronisation of an allocation. The
+ * workspace is a fixed array inside the library (about 18 MB per GPU that loads it, held
+ * until the process exits), so n is at most MPF_NOALLOC_MAX_MARKERS; larger n returns
+ * MPF_ERR_WORKSPACE before any device work. The first call on a device looks the array up
+ * (once per device, with that device current); make that first call before any stream
+ * capture. All calls share the array: calls that overlap on the GPU race. No counterpart
+ * in the reference.
+ */
+#define MPF_NOALLOC_MAX_MARKERS (1 << 20)
+MPF_API int mpf_sort_by_tile_noalloc(int kind, int degree, int ndim, const void* positions,
+                                     int64_t pos_stride, const void* values, int64_t val_stride,
+                                     int64_t ncomp, int64_t n, const double* lower,
+                                     const double* cell, const int32_t* num, const int32_t* code,
+                                     const int32_t* tile, int within, uint32_t* keys,
+                                     int32_t* order, int64_t* tile_start, int dtype, void* stream);
+
 /* The number of tiles of a grid for mpf_sort_by_tile, into *num_tiles. */
 MPF_API int mpf_num_tiles(int kind, int degree, int ndim, const int32_t* num, const int32_t* code,
                   const int32_t* tile, int64_t* num_tiles);

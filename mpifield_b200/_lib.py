@@ -61,6 +61,8 @@ _SIGNATURES = {
     "mpf_sort_workspace_bytes": ([_L, _L, _P], _I),
     "mpf_sort_by_tile": ([_I, _I, _I, _P, _L, _P, _L, _L, _L, _P, _P, _P, _P, _P, _I, _P, _P, _P, _P,
                           C.c_size_t, _I, _P], _I),
+    "mpf_sort_by_tile_noalloc": ([_I, _I, _I, _P, _L, _P, _L, _L, _L, _P, _P, _P, _P, _P, _I, _P, _P, _P, _I,
+                                  _P], _I),
     "mpf_permute_rows": ([_P, _L, _P, _L, _L, _P, _L, _I, _P], _I),
     "mpf_unpermute_rows": ([_P, _L, _P, _L, _L, _P, _L, _I, _P], _I),
 }

@@ -237,25 +237,26 @@ __global__ void unpermute_rows_kernel(T* dst, int64_t ds, const T* src, int64_t 
 
 // ------------------------------------------------------------------ host side --
 
-static int64_t sort_blocks(int64_t n) { return std::max<int64_t>(1, (n + kSortTile - 1) / kSortTile); }
-static int64_t scan_chunks(int64_t count) { return std::max<int64_t>(1, (count + kScanChunk - 1) / kScanChunk); }
-static size_t align256(size_t b) { return (b + 255) / 256 * 256; }
+constexpr int64_t sort_blocks(int64_t n) { return n > 0 ? (n + kSortTile - 1) / kSortTile : 1; }
+constexpr int64_t scan_chunks(int64_t count) { return count > 0 ? (count + kScanChunk - 1) / kScanChunk : 1; }
+constexpr size_t align256(size_t b) { return (b + 255) / 256 * 256; }
 
 struct SortLayout {
     size_t keys_a, keys_b, vals_a, vals_b, counts, sums, total;
 };
 
-static SortLayout sort_layout(int64_t n) {
-    SortLayout L;
+constexpr SortLayout sort_layout(int64_t n) {
     const int64_t nb = sort_blocks(n);
     const int64_t count = nb * (1 << 10);
+    const size_t items = align256(sizeof(uint32_t) * (size_t)(n > 0 ? n : 1));
+    SortLayout L{0, 0, 0, 0, 0, 0, 0};
     size_t off = 0;
-    L.keys_a = off; off += align256(sizeof(uint32_t) * std::max<int64_t>(n, 1));
-    L.keys_b = off; off += align256(sizeof(uint32_t) * std::max<int64_t>(n, 1));
-    L.vals_a = off; off += align256(sizeof(int32_t) * std::max<int64_t>(n, 1));
-    L.vals_b = off; off += align256(sizeof(int32_t) * std::max<int64_t>(n, 1));
-    L.counts = off; off += align256(sizeof(uint32_t) * count);
-    L.sums = off; off += align256(sizeof(uint32_t) * scan_chunks(count));
+    L.keys_a = off; off += items;
+    L.keys_b = off; off += items;
+    L.vals_a = off; off += items;
+    L.vals_b = off; off += items;
+    L.counts = off; off += align256(sizeof(uint32_t) * (size_t)count);
+    L.sums = off; off += align256(sizeof(uint32_t) * (size_t)scan_chunks(count));
     L.total = off;
     return L;
 }
@@ -402,7 +403,50 @@ int unpermute_rows(void* dst, int64_t ds, const void* src, int64_t ss, int64_t r
     return launch_status();
 }
 
+// ------------------------------------------------- the sort without allocation --
+//
+// Callers that cannot call cudaMalloc -- code recorded into a CUDA graph, where an
+// allocation may not be captured; a host application that owns every byte of device
+// memory through its own pool; a real-time loop that must not take the implicit device
+// synchronisation of an allocation -- sort through mpf_sort_by_tile_noalloc, whose
+// workspace is this file-scope array: every GPU that loads the library holds it (about
+// 18 MB) until the process exits, it keeps the last call's contents, and calls that
+// overlap on the GPU (two streams at once) race on it.
+
+constexpr int64_t kNoAllocMaxMarkers = MPF_NOALLOC_MAX_MARKERS;
+constexpr size_t kNoAllocBytes = sort_layout(kNoAllocMaxMarkers).total;
+
+static __device__ __align__(256) unsigned char g_noalloc_sort_scratch[kNoAllocBytes];
+
+// The device address of the array on the current device, looked up once per device.
+static void* noalloc_scratch() {
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= 64) return nullptr;
+    static void* address[64] = {nullptr};
+    if (!address[device]) {
+        void* p = nullptr;
+        if (record_cuda_error(cudaGetSymbolAddress(&p, g_noalloc_sort_scratch)) != MPF_OK) return nullptr;
+        address[device] = p;
+    }
+    return address[device];
+}
+
 template int tile_keys<double>(int, int, int, const KeyArgs<double>&, cudaStream_t);
 template int tile_keys<float>(int, int, int, const KeyArgs<float>&, cudaStream_t);
 
 }  // namespace mpf
+
+extern "C" int mpf_sort_by_tile_noalloc(int kind, int degree, int ndim, const void* positions, int64_t pos_stride,
+                                        const void* values, int64_t val_stride, int64_t ncomp, int64_t n,
+                                        const double* lower, const double* cell, const int32_t* num,
+                                        const int32_t* code, const int32_t* tile, int within, uint32_t* keys,
+                                        int32_t* order, int64_t* tile_start, int dtype, void* stream) {
+    // more markers than the array holds: refused before any device work
+    if (n > mpf::kNoAllocMaxMarkers) return MPF_ERR_WORKSPACE;
+    void* scratch = mpf::noalloc_scratch();
+    if (!scratch) return MPF_ERR_CUDA;
+    // no entry of the workspace needs a starting value: every pass writes what it reads
+    return mpf_sort_by_tile(kind, degree, ndim, positions, pos_stride, values, val_stride, ncomp, n, lower, cell,
+                            num, code, tile, within, keys, order, tile_start, scratch, mpf::kNoAllocBytes, dtype,
+                            stream);
+}
