@@ -71,6 +71,7 @@ typedef struct mpf_tuning {
     int32_t block;       /* threads per CTA (multiple of 32, <= 256); 0: default */
     int32_t smem_bytes;  /* dynamic shared memory per CTA for a box; 0: default */
     int32_t ctas_per_sm; /* resident CTAs per SM the grid is sized for; 0: default */
+    int32_t variant;     /* kernel variant; 0: the default for the shape (see mpf_gather, mpf_scatter) */
 } mpf_tuning;
 
 /* The library version, e.g. 10000 for 1.0.0. */

@@ -34,10 +34,10 @@ class BackendError(RuntimeError):
 
 
 class Tuning(C.Structure):
-    """``mpf_tuning``: the path, CTA size, shared memory and CTAs per SM of a launch."""
+    """``mpf_tuning``: the path, CTA size, shared memory, CTAs per SM and kernel variant of a launch."""
 
     _fields_ = [("path", C.c_int32), ("block", C.c_int32), ("smem_bytes", C.c_int32),
-                ("ctas_per_sm", C.c_int32)]
+                ("ctas_per_sm", C.c_int32), ("variant", C.c_int32)]
 
 
 _P = C.c_void_p
@@ -151,8 +151,9 @@ def geometry_arrays(geometry) -> tuple[C.Array, C.Array, C.Array, C.Array, int]:
     return lower, cell, num, code, ndim
 
 
-def tuning_struct(path: int = PATH_AUTO, block: int = 0, smem_bytes: int = 0, ctas_per_sm: int = 0) -> Tuning:
-    return Tuning(path, block, smem_bytes, ctas_per_sm)
+def tuning_struct(path: int = PATH_AUTO, block: int = 0, smem_bytes: int = 0, ctas_per_sm: int = 0,
+                  variant: int = 0) -> Tuning:
+    return Tuning(path, block, smem_bytes, ctas_per_sm, variant)
 
 
 def device_errors(clear: bool = True) -> int:

@@ -112,8 +112,9 @@ static int check_rows(const void* p, int64_t& stride, int64_t n, int rows, int d
 }
 
 static Tuning tuning_of(const mpf_tuning* t) {
-    Tuning u{0, 0, 0, 0};
+    Tuning u{0, 0, 0, 0, 0};
     if (t) {
+        u.variant = t->variant;
         u.path = t->path;
         u.block = t->block;
         u.smem_bytes = t->smem_bytes;

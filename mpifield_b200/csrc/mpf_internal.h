@@ -43,6 +43,7 @@ struct Tuning {
     int block;       // threads per CTA
     int smem_bytes;  // dynamic shared memory per CTA for the box
     int ctas_per_sm; // resident CTAs per SM the grid is sized for
+    int variant;     // kernel variant, 0 the default for the shape
 };
 
 template <typename T, int NDIM>

@@ -31,6 +31,10 @@ extern __shared__ __align__(16) unsigned char mpf_dynamic_smem[];
 
 constexpr int kMarkersPerThread = 4;
 constexpr int kMaxBlock = 256;
+// CTAs of 256 threads per SM the gather through L1 is register-bounded for.
+constexpr int kGatherMinBlocks = 3;
+// Consecutive markers per thread in the segment scatter.
+constexpr int kSegment = 8;
 
 template <typename T>
 __device__ __forceinline__ T rel_of(const NodeArgs<T>& a, int d, int64_t i) {
@@ -247,7 +251,9 @@ __device__ __forceinline__ bool box_holds(const Box& b, const int* lo, const int
 // `capacity` elements, so that the next chunks of the same cell tile fall inside it.
 // On a clamped-knot axis (no mapping) the box stays inside the array. Returns false
 // when not even the bare span fits.
-template <int NDIM, int S, typename G>
+// With ODD_LAST the last axis gets an odd extent where it can (one node more), so that
+// nodes of the box a whole number of rows apart fall in different shared-memory banks.
+template <int NDIM, int S, typename G, bool ODD_LAST = false>
 __device__ __forceinline__ bool choose_box(const int* lo, const int* hi, int ncomp, int capacity, const G& g,
                                            Box& b) {
     for (int margin = 2; margin >= 0; --margin) {
@@ -259,6 +265,10 @@ __device__ __forceinline__ bool choose_box(const int* lo, const int* hi, int nco
             if (g.code[d] == CLAMPED) {
                 first = max(first, 0);
                 end = min(end, g.ext[d]);
+            }
+            if (ODD_LAST && d == NDIM - 1 && ((end - first) & 1) == 0) {
+                if (g.code[d] != CLAMPED || end < g.ext[d]) ++end;
+                else if (first > 0) --first;
             }
             b.lo[d] = first;
             b.ex[d] = end - first;
@@ -491,6 +501,315 @@ __global__ void __launch_bounds__(kMaxBlock, 2) gather_kernel(const NodeArgs<T> 
 template <int S, int NDIM> struct StencilPoints {
     static constexpr int value = NDIM == 1 ? S : (NDIM == 2 ? S * S : S * S * S);
 };
+
+
+// The gather through L1: the positions of a chunk come by bulk copy as in gather_kernel,
+// and each marker reads its S^ndim nodes straight from global memory with 32-bit offsets
+// (the launcher uses it for fields of fewer than 2^31 entries), with no box and no
+// bounding pass: in a marker store sorted by cell, the nodes of consecutive markers stay
+// in L1. Bounded to MINB CTAs of 256 threads per SM.
+template <typename T, int NDIM, int KIND, int P, int NC, int MINB>
+__global__ void __launch_bounds__(kMaxBlock, MINB) gather_l1_kernel(const NodeArgs<T> a) {
+    constexpr int S = P + 1;
+    constexpr int NCC = NC > 0 ? NC : 1;
+    constexpr int MPT = kMarkersPerThread;
+    __shared__ __align__(8) uint64_t bars[2];
+    const int ncomp = NC > 0 ? NC : a.ncomp;
+    const int CH = MPT * blockDim.x;
+    T* posbuf = reinterpret_cast<T*>(mpf_dynamic_smem);  // [2][NDIM][CH]
+    const int64_t nchunks = (a.n + CH - 1) / CH;
+    int64_t c_first, c_last;
+    chunk_range(nchunks, c_first, c_last);
+    if (c_first >= c_last) return;
+    if (threadIdx.x == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        mbar_init_fence();
+    }
+    __syncthreads();
+    if (a.bulk && threadIdx.x == 0)
+        issue_positions<T, NDIM>(a, posbuf, CH, c_first * CH, (int)min((int64_t)CH, a.n - c_first * CH), &bars[0]);
+    const int sy = NDIM > 2 ? a.g.ext[2] : 1;
+    const int sx = NDIM > 1 ? a.g.ext[1] * sy : 1;
+    const int stride[3] = {NDIM == 1 ? 1 : sx, NDIM == 2 ? 1 : sy, 1};
+    for (int64_t ci = c_first; ci < c_last; ++ci) {
+        const int k = (int)(ci - c_first);
+        const int b = k & 1;
+        const int64_t first = ci * CH;
+        const int count = (int)min((int64_t)CH, a.n - first);
+        T* pb = posbuf + b * NDIM * CH;
+        if (a.bulk) {
+            if (threadIdx.x == 0 && ci + 1 < c_last) {
+                fence_proxy_async();
+                issue_positions<T, NDIM>(a, posbuf + (b ^ 1) * NDIM * CH, CH, first + CH,
+                                         (int)min((int64_t)CH, a.n - first - CH), &bars[b ^ 1]);
+            }
+            const bool late = !mbar_wait(&bars[b], (k >> 1) & 1);
+            if (__syncthreads_or(late)) {
+                if (threadIdx.x == 0) atomicOr(a.error, (unsigned)MPF_DEVICE_ERROR_WAIT);
+                if (threadIdx.x == 0 && ci + 1 < c_last) mbar_wait(&bars[b ^ 1], ((k + 1) >> 1) & 1);
+                __syncthreads();
+                return;
+            }
+        } else {
+            for (int j = threadIdx.x; j < count; j += blockDim.x)
+#pragma unroll
+                for (int d = 0; d < NDIM; ++d) pb[d * CH + j] = a.pos[d * a.pos_stride + first + j];
+            __syncthreads();
+        }
+#pragma unroll 1
+        for (int m = 0; m < MPT; ++m) {
+            const int j = m * blockDim.x + threadIdx.x;
+            if (j >= count) continue;
+            const int64_t i = first + j;
+            T w[3][S];
+            int off[3][S];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                if (d < NDIM) {
+                    const int base = axis_stencil<T, KIND, P>(rel_from(pb[d * CH + j], a.g, d), a.g.num[d],
+                                                              a.g.code[d], w[d]);
+#pragma unroll
+                    for (int s = 0; s < S; ++s) off[d][s] = map_node(base + s, a.g.num[d], a.g.code[d]) * stride[d];
+                } else {
+#pragma unroll
+                    for (int s = 0; s < S; ++s) {
+                        w[d][s] = T(s == 0);
+                        off[d][s] = 0;
+                    }
+                }
+            }
+            if constexpr (NC > 0) {
+                T acc[NCC];
+                stencil_sum<T, NDIM, S, NCC, true, int>(a.field_in, off, w, NC, 0, acc);
+#pragma unroll
+                for (int c = 0; c < NCC; ++c) a.result[c * a.res_stride + i] = acc[c];
+            } else {
+                for (int c = 0; c < ncomp; ++c) {
+                    T acc[1];
+                    stencil_sum<T, NDIM, S, 1, true, int>(a.field_in, off, w, ncomp, c, acc);
+                    a.result[c * a.res_stride + i] = acc[0];
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// 4- or 8-byte asynchronous copy global -> shared (cp.async, completion by group).
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(smem_u32(dst)), "l"(src), "n"(BYTES) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// The segment scatter of one component (stencils of at most 27 points). A chunk is
+// 256 x K consecutive markers; thread t owns the K markers t K .. t K + K - 1, which sit in
+// shared memory at t (K + 1) .. (a pitch of K + 1 keeps the lanes of a warp on distinct
+// banks at every step). The thread walks its markers in order and sums their weighted
+// contributions in registers while the stencil anchor stays the same; on a change of
+// anchor, and at the end of the segment, it adds the sum to the chunk's box in shared
+// memory (27 atomic adds per run instead of 27 per marker: markers of a cell are
+// consecutive in a store sorted by cell). At the end, lanes whose runs share an anchor --
+// the dense cells of a beam -- are summed across the warp first. Pass 1 turns each live
+// position into its cell coordinate in place and reduces the box; chunks whose box does
+// not fit add to global memory marker by marker.
+template <typename T, int NDIM, int KIND, int P>
+__global__ void __launch_bounds__(kMaxBlock, 2) scatter_segments_kernel(const NodeArgs<T> a) {
+    constexpr int S = P + 1;
+    constexpr int SY = NDIM > 1 ? S : 1;
+    constexpr int SZ = NDIM > 2 ? S : 1;
+    constexpr int SP = S * SY * SZ;
+    constexpr int K = kSegment;
+    constexpr int PITCH = K + 1;
+    constexpr int ROWS = NDIM + 1;
+    constexpr int CH = kMaxBlock * K;
+    constexpr int ROW = kMaxBlock * PITCH;
+    constexpr unsigned FULL = 0xffffffffu;
+    __shared__ int s_lo[3], s_hi[3];
+    T* buf = reinterpret_cast<T*>(mpf_dynamic_smem);  // [ROWS][ROW]
+    T* tile = buf + ROWS * ROW;
+    const int t = threadIdx.x;
+    const int lane = t & 31;
+    const int64_t nchunks = (a.n + CH - 1) / CH;
+    int64_t c_first, c_last;
+    chunk_range(nchunks, c_first, c_last);
+    Box box;
+    bool have_box = false;
+    for (int64_t ci = c_first; ci < c_last; ++ci) {
+        const int64_t first = ci * CH;
+        const int count = (int)min((int64_t)CH, a.n - first);
+        for (int j = t; j < count; j += kMaxBlock) {
+            const int q = (j / K) * PITCH + j % K;
+#pragma unroll
+            for (int d = 0; d < NDIM; ++d) cp_async<sizeof(T)>(buf + d * ROW + q, a.pos + d * a.pos_stride + first + j);
+            cp_async<sizeof(T)>(buf + NDIM * ROW + q, a.values + first + j);
+        }
+        cp_async_commit();
+        cp_async_wait_all();
+        __syncthreads();
+        // pass 1: cell coordinates in place, and the box of the live markers
+        const int nmine = min(K, max(0, count - t * K));
+        T* mine = buf + t * PITCH;
+        int lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
+#pragma unroll 1
+        for (int s = 0; s < nmine; ++s) {
+            if (mine[NDIM * ROW + s] == T(0)) continue;
+#pragma unroll
+            for (int d = 0; d < NDIM; ++d) {
+                const T rel = rel_from(mine[d * ROW + s], a.g, d);
+                mine[d * ROW + s] = rel;
+                T w[S];
+                const int base = axis_stencil<T, KIND, P>(rel, a.g.num[d], a.g.code[d], w);
+                lo[d] = min(lo[d], base);
+                hi[d] = max(hi[d], base);
+            }
+        }
+        bool staged = false;
+        if (!a.force_global) {
+            if (t < 3) {
+                s_lo[t] = INT_MAX;
+                s_hi[t] = INT_MIN;
+            }
+            __syncthreads();
+            block_box<NDIM>(lo, hi, s_lo, s_hi);
+            __syncthreads();
+            int clo[3], chi[3], top[3];
+            bool empty = false;
+#pragma unroll
+            for (int d = 0; d < NDIM; ++d) {
+                clo[d] = s_lo[d];
+                chi[d] = s_hi[d];
+                top[d] = chi[d] + S - 1;
+                if (chi[d] < clo[d]) empty = true;
+            }
+            if (empty) {  // every marker of the chunk is dead
+                __syncthreads();
+                continue;
+            }
+            if (have_box && box_holds<NDIM>(box, clo, top)) {
+                staged = true;
+            } else {
+                Box nb;
+                if (choose_box<NDIM, S, Grid<T>, true>(clo, chi, 1, a.capacity, a.g, nb)) {
+                    if (have_box) flush_box<T, NDIM, 1>(tile, a.field_out, box, a.g, 1);
+                    __syncthreads();
+                    int total = 1;
+#pragma unroll
+                    for (int d = 0; d < NDIM; ++d) total *= nb.ex[d];
+                    for (int q = t; q < total; q += kMaxBlock) tile[q] = T(0);
+                    __syncthreads();
+                    box = nb;
+                    have_box = true;
+                    staged = true;
+                }
+            }
+        }
+        if (staged) {
+            // box strides: node (a, b, e) of anchor key is tile[key + a sa + b sb + e se]
+            int st[3];
+            st[NDIM - 1] = 1;
+#pragma unroll
+            for (int d = NDIM - 2; d >= 0; --d) st[d] = st[d + 1] * box.ex[d + 1];
+            const int sa = st[0];
+            const int sb = NDIM > 1 ? st[1] : 0;
+            const int se = NDIM > 2 ? st[2] : 0;
+            T acc[SP];
+            int key = -1;  // the anchor of the open run, -1: none
+            auto flush = [&](int at) {
+#pragma unroll
+                for (int x = 0; x < S; ++x)
+#pragma unroll
+                    for (int y = 0; y < SY; ++y)
+#pragma unroll
+                        for (int z = 0; z < SZ; ++z)
+                            atomicAdd(tile + at + x * sa + y * sb + z * se, acc[(x * SY + y) * SZ + z]);
+            };
+#pragma unroll 1
+            for (int s = 0; s < nmine; ++s) {
+                const T v = mine[NDIM * ROW + s];
+                if (v == T(0)) continue;
+                T w[3][S];
+                int k = 0;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    if (d < NDIM) {
+                        const int base = axis_stencil<T, KIND, P>(mine[d * ROW + s], a.g.num[d], a.g.code[d], w[d]);
+                        k += (base - box.lo[d]) * st[d];
+                    } else {
+#pragma unroll
+                        for (int z = 0; z < S; ++z) w[d][z] = T(z == 0);
+                    }
+                }
+                const bool fresh = k != key;
+                if (fresh && key >= 0) flush(key);
+                T wz[SZ];
+#pragma unroll
+                for (int z = 0; z < SZ; ++z) wz[z] = (NDIM > 2 ? w[2][z] : T(1)) * v;
+#pragma unroll
+                for (int x = 0; x < S; ++x)
+#pragma unroll
+                    for (int y = 0; y < SY; ++y) {
+                        const T wxy = NDIM > 1 ? w[0][x] * w[1][y] : w[0][x];
+#pragma unroll
+                        for (int z = 0; z < SZ; ++z) {
+                            const T c = NDIM > 2 ? wxy * wz[z] : (NDIM > 1 ? w[0][x] * (w[1][y] * v) : w[0][x] * v);
+                            acc[(x * SY + y) * SZ + z] = fresh ? c : acc[(x * SY + y) * SZ + z] + c;
+                        }
+                    }
+                key = k;
+            }
+            // the closing runs: lanes of one anchor form contiguous groups in a sorted store;
+            // such groups are summed across the warp (a segmented suffix sum) before the adds
+            const int tag = key >= 0 ? key : -2 - lane;
+            const unsigned peers = __match_any_sync(FULL, tag);
+            const int head = __ffs(peers) - 1;
+            const int size = __popc(peers);
+            const int biggest = __reduce_max_sync(FULL, size);
+            const bool contiguous = peers == ((size == 32 ? FULL : ((1u << size) - 1u)) << head);
+            if (biggest >= 4 && __all_sync(FULL, contiguous)) {
+                const int last = head + size - 1;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+#pragma unroll
+                    for (int q = 0; q < SP; ++q) {
+                        const T other = __shfl_down_sync(FULL, acc[q], o);
+                        if (lane + o <= last) acc[q] += other;
+                    }
+                }
+                if (key >= 0 && lane == head) flush(key);
+            } else if (key >= 0) {
+                flush(key);
+            }
+        } else {
+            // no box: each live marker adds to global memory
+#pragma unroll 1
+            for (int s = 0; s < nmine; ++s) {
+                const T v = mine[NDIM * ROW + s];
+                if (v == T(0)) continue;
+                T w[3][S];
+                int base[3] = {0, 0, 0};
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    if (d < NDIM) {
+                        base[d] = axis_stencil<T, KIND, P>(mine[d * ROW + s], a.g.num[d], a.g.code[d], w[d]);
+                    } else {
+#pragma unroll
+                        for (int z = 0; z < S; ++z) w[d][z] = T(z == 0);
+                    }
+                }
+                int64_t off[3][S];
+                global_offsets<NDIM, S>(base, a.g.num, a.g.code, a.g.ext, off);
+                const T vv[1] = {v};
+                stencil_add<T, NDIM, S, 1, int64_t>(a.field_out, off, w, 1, 0, vv);
+            }
+        }
+        // the buffer and the box are free once every thread is past this point
+        __syncthreads();
+    }
+    if (have_box) flush_box<T, NDIM, 1>(tile, a.field_out, box, a.g, 1);
+}
 
 // The scatter. The markers of a chunk go to warps in contiguous runs of 32 (lane l of
 // warp w, step s: marker (w * MPT + s) * 32 + l of the chunk), so that in a marker store

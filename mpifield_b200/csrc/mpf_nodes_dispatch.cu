@@ -27,7 +27,7 @@ int launch_scatter(int kind, int degree, int ndim, const NodeArgs<T>& a, const T
 
 template <typename T>
 int launch_gather_grad(int kind, int degree, int ndim, const NodeArgs<T>& a, cudaStream_t s) {
-    return by_ndim<T>(2, kind, degree, ndim, a, Tuning{0, 0, 0, 0}, s);
+    return by_ndim<T>(2, kind, degree, ndim, a, Tuning{0, 0, 0, 0, 0}, s);
 }
 
 template int launch_gather<double>(int, int, int, const NodeArgs<double>&, const Tuning&, cudaStream_t);

@@ -26,40 +26,94 @@ static int pick_block(const Tuning& t) {
     return std::max(32, block / 32 * 32);
 }
 
-static unsigned grid_for(int64_t nchunks, int smem, int block) {
-    // two CTAs per SM at most (the kernels are bounded to 128 registers for that)
-    const int by_smem = std::max(1, (227 * 1024) / std::max(smem, 1));
-    const int per_sm = std::min({2, by_smem, 2048 / block});
+// CTAs for `nchunks` chunks: as many as fit on an SM by shared memory (1 KB reserved per
+// CTA), threads and the kernel's register bound (`max_per_sm`), times the SM count.
+static unsigned grid_for(int64_t nchunks, int smem, int block, int max_per_sm = 2) {
+    const int by_smem = std::max(1, (228 * 1024) / (smem + 1024 + 64));
+    const int per_sm = std::max(1, std::min({max_per_sm, by_smem, 2048 / block}));
     return (unsigned)std::max<int64_t>(1, std::min<int64_t>(nchunks, (int64_t)sm_count() * per_sm));
 }
 
+// Entries of the field (the gather through L1 indexes it with 32-bit offsets).
+template <typename T, int NDIM> static int64_t field_entries(const NodeArgs<T>& a) {
+    int64_t e = a.ncomp;
+    for (int d = 0; d < NDIM; ++d) e *= a.g.ext[d];
+    return e;
+}
+
+// Whether the position rows can be bulk-copied (16-byte aligned rows).
+template <typename T, int NDIM> static int bulk_positions(const NodeArgs<T>& a) {
+    const uintptr_t p = reinterpret_cast<uintptr_t>(a.pos);
+    return (p % 16 == 0) && (NDIM == 1 || (a.pos_stride * (int64_t)sizeof(T)) % 16 == 0) ? 1 : 0;
+}
+
+// Gather variants: 0 (default) through L1 while the field has fewer than 2^31 entries,
+// else with staged boxes; 1 staged boxes (path 1: global reads in that kernel); 2 through L1.
 template <typename T, int NDIM, int KIND, int P, int NC>
 static int run_gather(NodeArgs<T> a, const Tuning& t, cudaStream_t stream) {
-    const int block = pick_block(t);
+    const bool l1 = t.variant != 1 && field_entries<T, NDIM>(a) < ((int64_t)1 << 31);
+    const int block = l1 ? kMaxBlock : pick_block(t);
     const int CH = kMarkersPerThread * block;
-    const bool direct = t.path == 1;
+    const bool direct = t.path == 1 || l1;
     const int pos_bytes = 2 * NDIM * CH * (int)sizeof(T);
     int box_bytes = direct ? 0 : (t.smem_bytes > 0 ? t.smem_bytes : 48 * 1024);
     box_bytes = std::min(box_bytes, 227 * 1024 - pos_bytes);
     const int smem = pos_bytes + box_bytes;
     a.force_global = direct ? 1 : 0;
     a.capacity = box_bytes / (int)sizeof(T);
-    const uintptr_t p = reinterpret_cast<uintptr_t>(a.pos);
-    a.bulk = (p % 16 == 0) && (NDIM == 1 || (a.pos_stride * (int64_t)sizeof(T)) % 16 == 0) ? 1 : 0;
+    a.bulk = bulk_positions<T, NDIM>(a);
     a.error = device_error_word();
     if (!a.error) return MPF_ERR_CUDA;
-    auto kernel = gather_kernel<T, NDIM, KIND, P, NC>;
-    static int cache[64] = {0};
-    if (allow_smem(kernel, smem, cache) != MPF_OK) return MPF_ERR_CUDA;
     const int64_t nchunks = (a.n + CH - 1) / CH;
-    kernel<<<grid_for(nchunks, smem, block), block, smem, stream>>>(a);
+    if (l1) {
+        auto kernel = gather_l1_kernel<T, NDIM, KIND, P, NC, kGatherMinBlocks>;
+        static int cache[64] = {0};
+        if (allow_smem(kernel, smem, cache) != MPF_OK) return MPF_ERR_CUDA;
+        kernel<<<grid_for(nchunks, smem, block, kGatherMinBlocks), block, smem, stream>>>(a);
+    } else {
+        auto kernel = gather_kernel<T, NDIM, KIND, P, NC>;
+        static int cache[64] = {0};
+        if (allow_smem(kernel, smem, cache) != MPF_OK) return MPF_ERR_CUDA;
+        kernel<<<grid_for(nchunks, smem, block), block, smem, stream>>>(a);
+    }
     count_launches(1);
     return launch_status();
 }
 
+// The segment scatter (one component): 256 threads, a chunk of 256 x kSegment markers in
+// padded rows, and the box in the rest of half an SM's shared memory (or t.smem_bytes).
+template <typename T, int NDIM, int KIND, int P>
+static int run_scatter_segments(NodeArgs<T> a, const Tuning& t, cudaStream_t stream) {
+    const int buf_bytes = (NDIM + 1) * kMaxBlock * (kSegment + 1) * (int)sizeof(T);
+    const bool direct = t.path == 1;
+    int box_bytes = direct ? 0 : t.smem_bytes;
+    if (!direct && box_bytes <= 0) box_bytes = (228 * 1024) / 2 - 2048 - buf_bytes;  // two CTAs per SM
+    box_bytes = std::max(0, std::min(box_bytes, 227 * 1024 - buf_bytes));
+    const int smem = buf_bytes + box_bytes;
+    a.force_global = direct ? 1 : 0;
+    a.capacity = box_bytes / (int)sizeof(T);
+    a.bulk = 0;
+    a.error = device_error_word();
+    if (!a.error) return MPF_ERR_CUDA;
+    auto kernel = scatter_segments_kernel<T, NDIM, KIND, P>;
+    static int cache[64] = {0};
+    if (allow_smem(kernel, smem, cache) != MPF_OK) return MPF_ERR_CUDA;
+    const int CH = kMaxBlock * kSegment;
+    const int64_t nchunks = (a.n + CH - 1) / CH;
+    kernel<<<grid_for(nchunks, smem, kMaxBlock), kMaxBlock, smem, stream>>>(a);
+    count_launches(1);
+    return launch_status();
+}
+
+// Scatter variants: 0 (default) the segment scatter for one component and stencils of at
+// most 27 points, else the warp-transposed run reduction; 1 the segment scatter where it
+// applies; 2 the warp-transposed run reduction.
 template <typename T, int NDIM, int KIND, int P, int NC>
 static int run_scatter(NodeArgs<T> a, const Tuning& t, cudaStream_t stream) {
     constexpr int SP = StencilPoints<P + 1, NDIM>::value;
+    if constexpr (NC == 1 && SP <= 27) {
+        if (t.variant != 2) return run_scatter_segments<T, NDIM, KIND, P>(a, t, stream);
+    }
     constexpr int ROWS = SP < 32 ? SP : 32;
     const int block = pick_block(t);
     const int CH = kMarkersPerThread * block;

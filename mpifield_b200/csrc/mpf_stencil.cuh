@@ -25,12 +25,21 @@ template <> __device__ __forceinline__ int trunc_int<float>(float x) { return __
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
+// j modulo num in [0, num): one conditional add or subtract for the pre-mapping nodes of
+// a stencil (within a period of the grid), the integer remainder otherwise.
+__device__ __forceinline__ int wrap_index(int j, int num) {
+    if (j < 0) j += num;
+    else if (j >= num) j -= num;
+    if ((unsigned)j >= (unsigned)num) {
+        j %= num;
+        if (j < 0) j += num;
+    }
+    return j;
+}
+
 // Node index of pre-mapping node j on an axis of `num` nodes with boundary `code`.
 __device__ __forceinline__ int map_node(int j, int num, int code) {
-    if (code == PERIODIC) {
-        int m = j % num;
-        return m < 0 ? m + num : m;
-    }
+    if (code == PERIODIC) return wrap_index(j, num);
     if (code == BOUNDED) return clampi(j, 0, num - 1);
     return j;
 }
@@ -150,8 +159,7 @@ __device__ __forceinline__ int axis_stencil(T rel, int num, int code, T* w) {
         if (code == PERIODIC) {
             // for 0 < rel < num - 1 the quotient rel / num rounds below 1: the wrap is exact identity
             if (!(rel > T(0) && rel < T(num - 1))) rel = wrap_period(rel, num);
-            left = trunc_int<T>(rel) % num;
-            if (left < 0) left += num;
+            left = wrap_index(trunc_int<T>(rel), num);
         } else {
             left = rel >= T(0) ? trunc_int<T>(rel) : -1;
             left = clampi(left, 0, num - 2);

@@ -1,9 +1,10 @@
 """GPU parity of the node gather and scatter with the oracle (and the reference's fixtures).
 
 FP64 results agree with the oracle within RTOL_F64 = 1e-12 of max |oracle| (the
-atomic and summation order only); both launch paths (direct global memory, staged
-shared-memory boxes) are checked, on sorted and unsorted markers, periodic seams,
-bounded folds, clamped knots, dead markers, strided rows and the FP32 variant.
+atomic and summation order only); every kernel variant and launch path (direct global
+memory, staged shared-memory boxes, boxes too small) is checked, on sorted and unsorted
+markers, periodic seams, bounded folds, clamped knots, dense cells, dead markers,
+strided rows and the FP32 variant.
 """
 
 from __future__ import annotations
@@ -24,7 +25,20 @@ pytestmark = pytest.mark.gpu
 
 NODES = load("node_kernels.npz")
 DEV = "cuda"
-PATHS = {"direct": _lib.tuning_struct(_lib.PATH_DIRECT), "staged": _lib.tuning_struct(_lib.PATH_STAGED)}
+# Variant 0 is the default: the gather through L1, the segment scatter (one component,
+# at most 27 stencil points; direct: global atomics; small_box: boxes too small for most
+# chunks). Variant 1: the gather with staged boxes. Variant 2: the scatter's
+# warp-transposed run reduction (the default for the other shapes).
+PATHS = {"staged": _lib.tuning_struct(_lib.PATH_STAGED),
+         "direct": _lib.tuning_struct(_lib.PATH_DIRECT),
+         "small_box": _lib.tuning_struct(_lib.PATH_STAGED, smem_bytes=4096),
+         "boxed": _lib.tuning_struct(_lib.PATH_STAGED, variant=1),
+         "boxed_direct": _lib.tuning_struct(_lib.PATH_DIRECT, variant=1),
+         "boxed_small": _lib.tuning_struct(_lib.PATH_STAGED, smem_bytes=4096, variant=1),
+         "transposed": _lib.tuning_struct(_lib.PATH_STAGED, variant=2),
+         "transposed_small": _lib.tuning_struct(_lib.PATH_STAGED, smem_bytes=4096, variant=2)}
+GATHER_PATHS = ("staged", "boxed", "boxed_direct", "boxed_small")
+SCATTER_PATHS = ("staged", "direct", "small_box", "transposed", "transposed_small")
 
 
 def cu(a, dtype=torch.float64):
@@ -43,7 +57,7 @@ def run_scatter(kind, degree, pos, values, shape, geom, path="staged", dtype=tor
     return field.double().cpu().numpy()
 
 
-@pytest.mark.parametrize("path", ["direct", "staged"])
+@pytest.mark.parametrize("path", ["staged", "direct", "boxed", "transposed"])
 @pytest.mark.parametrize("tag", cases(NODES))
 def test_golden_cases(tag, path):
     kind, degree = node_case(tag)
@@ -80,8 +94,9 @@ def test_random_cases_sorted_and_unsorted(kind, degree, ndim):
             keys = np.floor((pos - np.array(geom[:ndim])[:, None]) / np.array(geom[ndim:2 * ndim])[:, None] / 4)
             order = np.lexsort(keys[::-1])
             for p, v, eg in ((pos, values, expected_g), (pos[:, order], values[:, order], expected_g[:, order])):
-                for path in ("direct", "staged"):
+                for path in GATHER_PATHS:
                     assert rel_err(run_gather(kind, degree, p, field, geom, path), eg) < RTOL_F64
+                for path in SCATTER_PATHS:
                     got = run_scatter(kind, degree, p, v, field.shape, geom, path)
                     assert rel_err(got, expected_s) < RTOL_F64
 
@@ -101,8 +116,27 @@ def test_large_sorted_3d_uses_the_boxes_and_agrees(kind, degree):
     ps, vs = pos[:, order], values[:, order]
     eg = O.gather(kind, degree, ps, field, geom)
     es = O.scatter(kind, degree, ps, vs, np.zeros((*shape, 1)), geom)
-    assert rel_err(run_gather(kind, degree, ps, field, geom), eg) < RTOL_F64
-    assert rel_err(run_scatter(kind, degree, ps, vs, (*shape, 1), geom), es) < RTOL_F64
+    for path in ("staged", "boxed"):
+        assert rel_err(run_gather(kind, degree, ps, field, geom, path), eg) < RTOL_F64
+    for path in ("staged", "transposed"):
+        assert rel_err(run_scatter(kind, degree, ps, vs, (*shape, 1), geom, path), es) < RTOL_F64
+
+
+@pytest.mark.parametrize("kind,degree,ndim", [("quadratic", 2, 3), ("linear", 1, 2), ("spline", 0, 3)])
+def test_dense_cells_sum_runs_across_the_warp(kind, degree, ndim):
+    # thousands of markers in a few cells, sorted: whole warps close runs of one anchor
+    rng = np.random.default_rng(6)
+    shape = (12, 10, 9)[:ndim]
+    geom = (*[0.0] * ndim, *[1.0] * ndim, *shape, *[1] * ndim)
+    n = 60_000
+    centres = np.array([[3.2, 4.7, 5.1], [3.6, 4.2, 5.9], [9.5, 0.1, 8.9]])[:, :ndim]
+    pick = np.sort(rng.integers(0, 3, n))
+    pos = (centres[pick] + rng.uniform(-0.05, 0.05, (n, ndim))).T.copy()
+    values = rng.uniform(0.5, 1.5, (1, n))
+    values[:, ::7] = 0.0
+    es = O.scatter(kind, degree, pos, values, np.zeros((*shape, 1)), geom)
+    for path in ("staged", "small_box", "transposed"):
+        assert rel_err(run_scatter(kind, degree, pos, values, (*shape, 1), geom, path), es) < RTOL_F64
 
 
 def test_strided_rows_and_noncontiguous_outputs():
