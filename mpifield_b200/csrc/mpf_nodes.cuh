@@ -33,8 +33,9 @@ constexpr int kMarkersPerThread = 4;
 constexpr int kMaxBlock = 256;
 // CTAs of 256 threads per SM the gather through L1 is register-bounded for.
 constexpr int kGatherMinBlocks = 3;
-// Consecutive markers per thread in the segment scatter.
+// Consecutive markers per thread in the segment scatter, and the widest margin of its boxes.
 constexpr int kSegment = 8;
+constexpr int kScatterMargin = 0;
 
 template <typename T>
 __device__ __forceinline__ T rel_of(const NodeArgs<T>& a, int d, int64_t i) {
@@ -253,10 +254,10 @@ __device__ __forceinline__ bool box_holds(const Box& b, const int* lo, const int
 // when not even the bare span fits.
 // With ODD_LAST the last axis gets an odd extent where it can (one node more), so that
 // nodes of the box a whole number of rows apart fall in different shared-memory banks.
-template <int NDIM, int S, typename G, bool ODD_LAST = false>
+template <int NDIM, int S, typename G, bool ODD_LAST = false, int MAX_MARGIN = 2>
 __device__ __forceinline__ bool choose_box(const int* lo, const int* hi, int ncomp, int capacity, const G& g,
                                            Box& b) {
-    for (int margin = 2; margin >= 0; --margin) {
+    for (int margin = MAX_MARGIN; margin >= 0; --margin) {
         int64_t vol = ncomp;
 #pragma unroll
         for (int d = 0; d < NDIM; ++d) {
@@ -508,13 +509,15 @@ template <int S, int NDIM> struct StencilPoints {
 // (the launcher uses it for fields of fewer than 2^31 entries), with no box and no
 // bounding pass: in a marker store sorted by cell, the nodes of consecutive markers stay
 // in L1. Bounded to MINB CTAs of 256 threads per SM.
-template <typename T, int NDIM, int KIND, int P, int NC, int MINB>
+template <typename T, int NDIM, int KIND, int P, int NC, int MINB, int UNI>
 __global__ void __launch_bounds__(kMaxBlock, MINB) gather_l1_kernel(const NodeArgs<T> a) {
     constexpr int S = P + 1;
     constexpr int NCC = NC > 0 ? NC : 1;
     constexpr int MPT = kMarkersPerThread;
     __shared__ __align__(8) uint64_t bars[2];
     const int ncomp = NC > 0 ? NC : a.ncomp;
+    // UNI >= 0: every axis has that boundary code (a compile-time constant)
+    auto code = [&](int d) { return UNI >= 0 ? UNI : a.g.code[d]; };
     const int CH = MPT * blockDim.x;
     T* posbuf = reinterpret_cast<T*>(mpf_dynamic_smem);  // [2][NDIM][CH]
     const int64_t nchunks = (a.n + CH - 1) / CH;
@@ -568,9 +571,9 @@ __global__ void __launch_bounds__(kMaxBlock, MINB) gather_l1_kernel(const NodeAr
             for (int d = 0; d < 3; ++d) {
                 if (d < NDIM) {
                     const int base = axis_stencil<T, KIND, P>(rel_from(pb[d * CH + j], a.g, d), a.g.num[d],
-                                                              a.g.code[d], w[d]);
+                                                              code(d), w[d]);
 #pragma unroll
-                    for (int s = 0; s < S; ++s) off[d][s] = map_node(base + s, a.g.num[d], a.g.code[d]) * stride[d];
+                    for (int s = 0; s < S; ++s) off[d][s] = map_node(base + s, a.g.num[d], code(d)) * stride[d];
                 } else {
 #pragma unroll
                     for (int s = 0; s < S; ++s) {
@@ -615,21 +618,29 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // the dense cells of a beam -- are summed across the warp first. Pass 1 turns each live
 // position into its cell coordinate in place and reduces the box; chunks whose box does
 // not fit add to global memory marker by marker.
-template <typename T, int NDIM, int KIND, int P>
-__global__ void __launch_bounds__(kMaxBlock, 2) scatter_segments_kernel(const NodeArgs<T> a) {
+template <typename T, int NDIM, int KIND, int P, int K, int MINB, int UNI>
+__global__ void __launch_bounds__(kMaxBlock, MINB) scatter_segments_kernel(const NodeArgs<T> a) {
     constexpr int S = P + 1;
     constexpr int SY = NDIM > 1 ? S : 1;
     constexpr int SZ = NDIM > 2 ? S : 1;
     constexpr int SP = S * SY * SZ;
-    constexpr int K = kSegment;
     constexpr int PITCH = K + 1;
     constexpr int ROWS = NDIM + 1;
     constexpr int CH = kMaxBlock * K;
     constexpr int ROW = kMaxBlock * PITCH;
     constexpr unsigned FULL = 0xffffffffu;
-    __shared__ int s_lo[3], s_hi[3];
+    // UNI >= 0: every axis has that boundary code (a compile-time constant)
+    auto code = [&](int d) { return UNI >= 0 ? UNI : a.g.code[d]; };
+    __shared__ int s_lo[3], s_hi[3], s_lo2[3], s_hi2[3];
     T* buf = reinterpret_cast<T*>(mpf_dynamic_smem);  // [ROWS][ROW]
     T* tile = buf + ROWS * ROW;
+    // A periodic axis can also be measured in a frame shifted by half a period (anchor a
+    // as ((a + half) mod num) + num - half, the same node modulo num): a chunk that
+    // crosses the seam of the grid -- the last and the first tiles of a row -- has a short
+    // span in that frame. The box takes whichever frame is shorter, per axis.
+    int half[3], shifted[3] = {0, 0, 0};
+#pragma unroll
+    for (int d = 0; d < NDIM; ++d) half[d] = a.g.num[d] / 2;
     const int t = threadIdx.x;
     const int lane = t & 31;
     const int64_t nchunks = (a.n + CH - 1) / CH;
@@ -653,6 +664,7 @@ __global__ void __launch_bounds__(kMaxBlock, 2) scatter_segments_kernel(const No
         const int nmine = min(K, max(0, count - t * K));
         T* mine = buf + t * PITCH;
         int lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
+        int lo2[3] = {INT_MAX, INT_MAX, INT_MAX}, hi2[3] = {INT_MIN, INT_MIN, INT_MIN};
 #pragma unroll 1
         for (int s = 0; s < nmine; ++s) {
             if (mine[NDIM * ROW + s] == T(0)) continue;
@@ -661,9 +673,12 @@ __global__ void __launch_bounds__(kMaxBlock, 2) scatter_segments_kernel(const No
                 const T rel = rel_from(mine[d * ROW + s], a.g, d);
                 mine[d * ROW + s] = rel;
                 T w[S];
-                const int base = axis_stencil<T, KIND, P>(rel, a.g.num[d], a.g.code[d], w);
+                const int base = axis_stencil<T, KIND, P>(rel, a.g.num[d], code(d), w);
                 lo[d] = min(lo[d], base);
                 hi[d] = max(hi[d], base);
+                const int moved = wrap_index(base + half[d], a.g.num[d]);
+                lo2[d] = min(lo2[d], moved);
+                hi2[d] = max(hi2[d], moved);
             }
         }
         bool staged = false;
@@ -671,16 +686,24 @@ __global__ void __launch_bounds__(kMaxBlock, 2) scatter_segments_kernel(const No
             if (t < 3) {
                 s_lo[t] = INT_MAX;
                 s_hi[t] = INT_MIN;
+                s_lo2[t] = INT_MAX;
+                s_hi2[t] = INT_MIN;
             }
             __syncthreads();
             block_box<NDIM>(lo, hi, s_lo, s_hi);
+            block_box<NDIM>(lo2, hi2, s_lo2, s_hi2);
             __syncthreads();
-            int clo[3], chi[3], top[3];
+            int clo[3], chi[3], top[3], frame[3] = {0, 0, 0};
             bool empty = false;
 #pragma unroll
             for (int d = 0; d < NDIM; ++d) {
                 clo[d] = s_lo[d];
                 chi[d] = s_hi[d];
+                if (code(d) == PERIODIC && s_hi2[d] - s_lo2[d] < chi[d] - clo[d]) {
+                    frame[d] = 1;
+                    clo[d] = s_lo2[d] + a.g.num[d] - half[d];
+                    chi[d] = s_hi2[d] + a.g.num[d] - half[d];
+                }
                 top[d] = chi[d] + S - 1;
                 if (chi[d] < clo[d]) empty = true;
             }
@@ -688,11 +711,14 @@ __global__ void __launch_bounds__(kMaxBlock, 2) scatter_segments_kernel(const No
                 __syncthreads();
                 continue;
             }
-            if (have_box && box_holds<NDIM>(box, clo, top)) {
+            bool same_frame = true;
+#pragma unroll
+            for (int d = 0; d < NDIM; ++d) same_frame = same_frame && frame[d] == shifted[d];
+            if (have_box && same_frame && box_holds<NDIM>(box, clo, top)) {
                 staged = true;
             } else {
                 Box nb;
-                if (choose_box<NDIM, S, Grid<T>, true>(clo, chi, 1, a.capacity, a.g, nb)) {
+                if (choose_box<NDIM, S, Grid<T>, true, kScatterMargin>(clo, chi, 1, a.capacity, a.g, nb)) {
                     if (have_box) flush_box<T, NDIM, 1>(tile, a.field_out, box, a.g, 1);
                     __syncthreads();
                     int total = 1;
@@ -701,6 +727,8 @@ __global__ void __launch_bounds__(kMaxBlock, 2) scatter_segments_kernel(const No
                     for (int q = t; q < total; q += kMaxBlock) tile[q] = T(0);
                     __syncthreads();
                     box = nb;
+#pragma unroll
+                    for (int d = 0; d < NDIM; ++d) shifted[d] = frame[d];
                     have_box = true;
                     staged = true;
                 }
@@ -716,15 +744,20 @@ __global__ void __launch_bounds__(kMaxBlock, 2) scatter_segments_kernel(const No
             const int sb = NDIM > 1 ? st[1] : 0;
             const int se = NDIM > 2 ? st[2] : 0;
             T acc[SP];
+#pragma unroll
+            for (int q = 0; q < SP; ++q) acc[q] = T(0);
             int key = -1;  // the anchor of the open run, -1: none
+            // adds the open run to the box and empties it
             auto flush = [&](int at) {
 #pragma unroll
                 for (int x = 0; x < S; ++x)
 #pragma unroll
                     for (int y = 0; y < SY; ++y)
 #pragma unroll
-                        for (int z = 0; z < SZ; ++z)
+                        for (int z = 0; z < SZ; ++z) {
                             atomicAdd(tile + at + x * sa + y * sb + z * se, acc[(x * SY + y) * SZ + z]);
+                            acc[(x * SY + y) * SZ + z] = T(0);
+                        }
             };
 #pragma unroll 1
             for (int s = 0; s < nmine; ++s) {
@@ -735,15 +768,15 @@ __global__ void __launch_bounds__(kMaxBlock, 2) scatter_segments_kernel(const No
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
                     if (d < NDIM) {
-                        const int base = axis_stencil<T, KIND, P>(mine[d * ROW + s], a.g.num[d], a.g.code[d], w[d]);
+                        int base = axis_stencil<T, KIND, P>(mine[d * ROW + s], a.g.num[d], code(d), w[d]);
+                        if (shifted[d]) base = wrap_index(base + half[d], a.g.num[d]) + a.g.num[d] - half[d];
                         k += (base - box.lo[d]) * st[d];
                     } else {
 #pragma unroll
                         for (int z = 0; z < S; ++z) w[d][z] = T(z == 0);
                     }
                 }
-                const bool fresh = k != key;
-                if (fresh && key >= 0) flush(key);
+                if (k != key && key >= 0) flush(key);
                 T wz[SZ];
 #pragma unroll
                 for (int z = 0; z < SZ; ++z) wz[z] = (NDIM > 2 ? w[2][z] : T(1)) * v;
@@ -751,11 +784,11 @@ __global__ void __launch_bounds__(kMaxBlock, 2) scatter_segments_kernel(const No
                 for (int x = 0; x < S; ++x)
 #pragma unroll
                     for (int y = 0; y < SY; ++y) {
-                        const T wxy = NDIM > 1 ? w[0][x] * w[1][y] : w[0][x];
+                        const T wxy = NDIM > 2 ? w[0][x] * w[1][y] : (NDIM > 1 ? w[0][x] * (w[1][y] * v) : w[0][x] * v);
 #pragma unroll
                         for (int z = 0; z < SZ; ++z) {
-                            const T c = NDIM > 2 ? wxy * wz[z] : (NDIM > 1 ? w[0][x] * (w[1][y] * v) : w[0][x] * v);
-                            acc[(x * SY + y) * SZ + z] = fresh ? c : acc[(x * SY + y) * SZ + z] + c;
+                            T& r = acc[(x * SY + y) * SZ + z];
+                            r = NDIM > 2 ? fma(wxy, wz[z], r) : r + wxy;
                         }
                     }
                 key = k;
@@ -793,7 +826,7 @@ __global__ void __launch_bounds__(kMaxBlock, 2) scatter_segments_kernel(const No
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
                     if (d < NDIM) {
-                        base[d] = axis_stencil<T, KIND, P>(mine[d * ROW + s], a.g.num[d], a.g.code[d], w[d]);
+                        base[d] = axis_stencil<T, KIND, P>(mine[d * ROW + s], a.g.num[d], code(d), w[d]);
                     } else {
 #pragma unroll
                         for (int z = 0; z < S; ++z) w[d][z] = T(z == 0);

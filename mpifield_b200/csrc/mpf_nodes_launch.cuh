@@ -41,6 +41,13 @@ template <typename T, int NDIM> static int64_t field_entries(const NodeArgs<T>& 
     return e;
 }
 
+// Whether every axis is periodic (the kernels then take the code as a constant).
+template <typename T, int NDIM> static bool all_periodic(const NodeArgs<T>& a) {
+    for (int d = 0; d < NDIM; ++d)
+        if (a.g.code[d] != PERIODIC) return false;
+    return true;
+}
+
 // Whether the position rows can be bulk-copied (16-byte aligned rows).
 template <typename T, int NDIM> static int bulk_positions(const NodeArgs<T>& a) {
     const uintptr_t p = reinterpret_cast<uintptr_t>(a.pos);
@@ -66,7 +73,9 @@ static int run_gather(NodeArgs<T> a, const Tuning& t, cudaStream_t stream) {
     if (!a.error) return MPF_ERR_CUDA;
     const int64_t nchunks = (a.n + CH - 1) / CH;
     if (l1) {
-        auto kernel = gather_l1_kernel<T, NDIM, KIND, P, NC, kGatherMinBlocks>;
+        // (the boundary codes stay run-time values here: a periodic-only build of this kernel
+        // measured slower)
+        auto kernel = gather_l1_kernel<T, NDIM, KIND, P, NC, kGatherMinBlocks, -1>;
         static int cache[64] = {0};
         if (allow_smem(kernel, smem, cache) != MPF_OK) return MPF_ERR_CUDA;
         kernel<<<grid_for(nchunks, smem, block, kGatherMinBlocks), block, smem, stream>>>(a);
@@ -80,14 +89,14 @@ static int run_gather(NodeArgs<T> a, const Tuning& t, cudaStream_t stream) {
     return launch_status();
 }
 
-// The segment scatter (one component): 256 threads, a chunk of 256 x kSegment markers in
-// padded rows, and the box in the rest of half an SM's shared memory (or t.smem_bytes).
-template <typename T, int NDIM, int KIND, int P>
+// The segment scatter (one component): 256 threads, a chunk of 256 x K markers in padded
+// rows, MINB CTAs per SM, the box in the rest of the SM's shared memory (or t.smem_bytes).
+template <typename T, int NDIM, int KIND, int P, int K, int MINB>
 static int run_scatter_segments(NodeArgs<T> a, const Tuning& t, cudaStream_t stream) {
-    const int buf_bytes = (NDIM + 1) * kMaxBlock * (kSegment + 1) * (int)sizeof(T);
+    const int buf_bytes = (NDIM + 1) * kMaxBlock * (K + 1) * (int)sizeof(T);
     const bool direct = t.path == 1;
     int box_bytes = direct ? 0 : t.smem_bytes;
-    if (!direct && box_bytes <= 0) box_bytes = (228 * 1024) / 2 - 2048 - buf_bytes;  // two CTAs per SM
+    if (!direct && box_bytes <= 0) box_bytes = (228 * 1024) / MINB - 2048 - buf_bytes;
     box_bytes = std::max(0, std::min(box_bytes, 227 * 1024 - buf_bytes));
     const int smem = buf_bytes + box_bytes;
     a.force_global = direct ? 1 : 0;
@@ -95,12 +104,14 @@ static int run_scatter_segments(NodeArgs<T> a, const Tuning& t, cudaStream_t str
     a.bulk = 0;
     a.error = device_error_word();
     if (!a.error) return MPF_ERR_CUDA;
-    auto kernel = scatter_segments_kernel<T, NDIM, KIND, P>;
-    static int cache[64] = {0};
-    if (allow_smem(kernel, smem, cache) != MPF_OK) return MPF_ERR_CUDA;
-    const int CH = kMaxBlock * kSegment;
+    const bool per = all_periodic<T, NDIM>(a);
+    auto kernel = per ? scatter_segments_kernel<T, NDIM, KIND, P, K, MINB, PERIODIC>
+                      : scatter_segments_kernel<T, NDIM, KIND, P, K, MINB, -1>;
+    static int cache[2][64] = {{0}};
+    if (allow_smem(kernel, smem, cache[per]) != MPF_OK) return MPF_ERR_CUDA;
+    const int CH = kMaxBlock * K;
     const int64_t nchunks = (a.n + CH - 1) / CH;
-    kernel<<<grid_for(nchunks, smem, kMaxBlock), kMaxBlock, smem, stream>>>(a);
+    kernel<<<grid_for(nchunks, smem, kMaxBlock, MINB), kMaxBlock, smem, stream>>>(a);
     count_launches(1);
     return launch_status();
 }
@@ -112,7 +123,8 @@ template <typename T, int NDIM, int KIND, int P, int NC>
 static int run_scatter(NodeArgs<T> a, const Tuning& t, cudaStream_t stream) {
     constexpr int SP = StencilPoints<P + 1, NDIM>::value;
     if constexpr (NC == 1 && SP <= 27) {
-        if (t.variant != 2) return run_scatter_segments<T, NDIM, KIND, P>(a, t, stream);
+        if (t.variant == 3) return run_scatter_segments<T, NDIM, KIND, P, 4, 3>(a, t, stream);
+        if (t.variant != 2) return run_scatter_segments<T, NDIM, KIND, P, kSegment, 2>(a, t, stream);
     }
     constexpr int ROWS = SP < 32 ? SP : 32;
     const int block = pick_block(t);
