@@ -65,6 +65,7 @@ def parse() -> argparse.Namespace:
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-ref-cuda", action="store_true")
+    p.add_argument("--no-extras", action="store_true", help="skip the other configurations' measurements")
     return p.parse_args()
 
 
@@ -442,6 +443,16 @@ def run_ours(args, world, rank, local) -> None:
     if not args.no_cpu and rank == 0 and world == 1:
         cpu = cpu_baseline(1 << 21)
 
+    extras = {}
+    if not args.no_extras and rank == 0 and world == 1 and dtype == torch.float64:
+        reps = max(2, args.steps // 2)
+        extras["fp32_variant"] = measure_fp32(step, ps, ws, reps)
+        extras["plain_2d"] = measure_plain_2d(device, max(10, args.steps))
+        del pos, w
+        torch.cuda.empty_cache()
+        extras["autograd"] = measure_autograd(device, reps)
+        extras["path_deposit"] = measure_paths(device, reps, peak)
+
     clock = clocks.summary()
     if rank == 0:
         line = {
@@ -465,7 +476,166 @@ def run_ours(args, world, rank, local) -> None:
             "cpu_baseline": cpu, "ref_cuda": ref_cuda, "e2e": e2e, "gpu_launches": int(launches),
             "clocks": clock,
         }
+        line.update(extras)
         print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------ the other configurations --
+#
+# Reported beside the headline in the same JSON line (keys "fp32_variant", "path_deposit",
+# "autograd", "plain_2d"); each is a short measurement of its own configuration with
+# CUDA events on the current stream.
+
+def _event_ms(fn, reps: int) -> float:
+    fn()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(reps):
+        fn()
+    b.record()
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / reps
+
+
+def measure_fp32(step, ps, ws, reps: int) -> dict:
+    """The float32 variant of the headline step on the same sorted store, and its error
+    against the float64 results (max |f32 - f64| / max |f64|, per output)."""
+    import mpifield_b200 as mf
+
+    n = ps.shape[1]
+    step.gather_scatter(ps, ws)
+    E64, D64 = step.E.clone(), step.density.clone()
+    p32, w32, f32 = ps.float(), ws.float(), step.field.float()
+    E32 = torch.empty((3, n), dtype=torch.float32, device=ps.device)
+    D32 = torch.zeros(step.density.shape, dtype=torch.float32, device=ps.device)
+    gather, scatter = mf.KERNELS["gather_quadratic_3d"], mf.KERNELS["scatter_quadratic_3d"]
+
+    def go():
+        gather(p32, f32, E32, *step.geom)
+        D32.zero_()
+        scatter(p32, w32, D32, *step.geom)
+
+    ms = _event_ms(go, reps)
+    err_e = float((E32.double() - E64).abs().max() / E64.abs().max())
+    err_d = float((D32.double() - D64).abs().max() / D64.abs().max())
+    del p32, w32, f32, E32, D32, E64, D64
+    return {"value": n / (ms / 1000.0), "unit": "markers/s", "ms_per_step": ms,
+            "max_rel_err_vs_f64": {"gather": err_e, "scatter": err_d},
+            "what": "gather + scatter in float32 on the same store (positions, weights and field rounded "
+                    "to float32); error relative to max |float64 result|"}
+
+
+def measure_paths(device, reps: int, peak: float) -> dict:
+    """The path deposit: 128^3 periodic, N = 2^25 paths, start uniform, end = start +
+    U[-0.9, 0.9] cells per axis, charges U[0.5, 1.5]; WHITNEY and QUADRATIC_EDGES, paths in
+    random order and sorted by the start's cell tile; continuity residual
+    max |rho(end) - rho(start) - G^T J| with the node deposit of the same degree."""
+    import mpifield_b200 as mf
+
+    n, g_n = 1 << 25, 128
+    g = torch.Generator(device=device).manual_seed(7)
+    start = torch.rand((3, n), generator=g, device=device, dtype=torch.float64)
+    end = start + (torch.rand((3, n), generator=g, device=device, dtype=torch.float64) * 1.8 - 0.9) / g_n
+    q = torch.rand((1, n), generator=g, device=device, dtype=torch.float64) + 0.5
+    grid = mf.BlockGrid.from_geometry((0.0,) * 3, (1.0 / g_n,) * 3, (g_n,) * 3, (True,) * 3)
+    geom = grid.geometry
+    t = mf.sort_by_tile(start, mf.LINEAR, geom, TILE, within=True)
+    s_start, s_end, s_q = mf.permute(start, t.order), mf.permute(end, t.order), mf.permute(q, t.order)
+    edges = torch.zeros((g_n, g_n, g_n, 3), dtype=torch.float64, device=device)
+    nbytes = n * 56 + g_n ** 3 * 24 * 2
+    out = {"config": f"{g_n}^3 periodic, N={n} paths, |displacement| <= 0.9 cell per axis", "unit": "paths/s",
+           "algorithmic_bytes": nbytes}
+    for degree, name in ((1, "whitney"), (2, "quadratic_edges")):
+        ew, nodes = mf.splines(degree).edges, mf.splines(degree).nodes
+        res = {}
+        for order, (a, b, c) in (("random", (start, end, q)), ("sorted", (s_start, s_end, s_q))):
+            def go():
+                edges.zero_()
+                ew.deposit_paths_block(a, b, c[0], edges, grid)
+            ms = _event_ms(go, reps)
+            res[order] = {"value": n / (ms / 1000.0), "ms": ms,
+                          "hbm_frac": nbytes / (ms / 1000.0) / 1e9 / peak}
+        before = torch.zeros((g_n, g_n, g_n, 1), dtype=torch.float64, device=device)
+        after = torch.zeros_like(before)
+        nodes.scatter_block(start, q[0], before, grid)
+        nodes.scatter_block(end, q[0], after, grid)
+        edges.zero_()
+        ew.deposit_paths_block(start, end, q[0], edges, grid)
+        change = (after - before)[..., 0]
+        resid = float((ew.divergence_block(edges, grid) - change).abs().max())
+        res["continuity_residual"] = resid
+        res["continuity_scale"] = float(change.abs().max())
+        out[name] = res
+        del before, after, change
+    return out
+
+
+def measure_autograd(device, reps: int) -> dict:
+    """Differentiation: 512^2 periodic, CUBIC, 1-component field of seeded Fourier modes,
+    N = 2^22 uniform markers, weights U[0, 1]; forward + backward of
+    sum(w gather(f, x)) + 0.5 ||scatter(x, w)||^2 with respect to f, w and x."""
+    import mpifield_b200 as mf
+    from mpifield_b200 import autograd as AG
+
+    n, g_n = 1 << 22, 512
+    geom = (0.0, 0.0, 1.0 / g_n, 1.0 / g_n, g_n, g_n, 1, 1)
+    gen = torch.Generator(device="cpu").manual_seed(5)
+    xs = torch.arange(g_n, dtype=torch.float64) / g_n
+    f0 = torch.zeros((g_n, g_n), dtype=torch.float64)
+    for _ in range(8):
+        k = torch.randint(1, 9, (2,), generator=gen)
+        phase = float(torch.rand(1, generator=gen)) * 2 * np.pi
+        f0 += torch.cos(2 * np.pi * (k[0] * xs[:, None] + k[1] * xs[None, :]) + phase)
+    g = torch.Generator(device=device).manual_seed(6)
+    x0 = torch.rand((2, n), generator=g, device=device, dtype=torch.float64)
+    w0 = torch.rand((1, n), generator=g, device=device, dtype=torch.float64)
+    out = {"config": f"{g_n}^2 periodic, CUBIC, N={n}", "unit": "markers/s"}
+    for dtype, name in ((torch.float64, "f64"), (torch.float32, "f32")):
+        f = f0.to(device=device, dtype=dtype).view(g_n, g_n, 1).clone().requires_grad_(True)
+        w = w0.to(dtype).clone().requires_grad_(True)
+        x = x0.to(dtype).clone().requires_grad_(True)
+
+        def go():
+            f.grad = w.grad = x.grad = None
+            rho = AG.scatter(x, w, mf.CUBIC, geom)
+            loss = (w * AG.gather(f, x, mf.CUBIC, geom)).sum() + 0.5 * (rho * rho).sum()
+            loss.backward()
+
+        ms = _event_ms(go, reps)
+        out[name] = {"value": n / (ms / 1000.0), "ms_per_step": ms}
+    return out
+
+
+def measure_plain_2d(device, reps: int) -> dict:
+    """The plain 2D configuration: 101 x 51 nodes on [0, 0.1] x [0, 0.05], bounded; LINEAR;
+    E = -gradient(phi), phi = 1000 exp(-((x - 0.05)^2 + (y - 0.025)^2) / 1e-4); N = 100,000
+    uniform markers (numpy default_rng(0)); scatter unit weights + gather E (2, N). The
+    kernels on the block itself (its halo nodes trimmed at the bounded walls)."""
+    import mpifield_b200 as mf
+
+    nx, ny, n = 101, 51, 100_000
+    hx, hy = 0.1 / (nx - 1), 0.05 / (ny - 1)
+    geom = (0.0, 0.0, hx, hy, nx, ny, 0, 0)
+    X, Y = np.meshgrid(np.linspace(0, 0.1, nx), np.linspace(0, 0.05, ny), indexing="ij")
+    phi = 1000.0 * np.exp(-((X - 0.05) ** 2 + (Y - 0.025) ** 2) / 1e-4)
+    ex, ey = np.gradient(phi, hx, hy)
+    E = torch.tensor(np.stack([-ex, -ey], axis=-1), device=device)
+    rng = np.random.default_rng(0)
+    pos = torch.tensor(np.stack([rng.uniform(0, 0.1, n), rng.uniform(0, 0.05, n)]), device=device)
+    ones = torch.ones((1, n), dtype=torch.float64, device=device)
+    rho = torch.zeros((nx, ny, 1), dtype=torch.float64, device=device)
+    out_e = torch.empty((2, n), dtype=torch.float64, device=device)
+    gather, scatter = mf.KERNELS["gather_linear_2d"], mf.KERNELS["scatter_linear_2d"]
+
+    def go():
+        rho.zero_()
+        scatter(pos, ones, rho, *geom)
+        gather(pos, E, out_e, *geom)
+
+    ms = _event_ms(go, reps)
+    return {"value": n / (ms / 1000.0), "unit": "markers/s", "us_per_step": ms * 1000.0,
+            "config": "101x51 bounded, LINEAR, N=100000: scatter + gather (launch-bound)"}
 
 
 def run_reference(args, world, rank) -> None:
