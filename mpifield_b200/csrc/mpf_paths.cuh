@@ -340,15 +340,41 @@ __device__ void spline_path(T q, const T* r0, const T* r1, const Grid<T>& g, con
                     p0[d] = begin;
                     step[d] = finish - begin;
                 }
+                // The Gauss points of a piece lie in one knot interval on every axis, so
+                // they share the edges of their stencils: their contributions are summed
+                // in registers and added once per piece and axis (a point whose stencil
+                // differs -- rounding at a cut -- closes the sum and opens a new one).
+                constexpr int SX = P + 1;
+                constexpr int CNT = P * (NDIM > 1 ? SX : 1) * (NDIM > 2 ? SX : 1);
 #pragma unroll
-                for (int gp = 0; gp < NPTS; ++gp) {
-                    const T point = Gauss<T, NPTS>::point(gp);
-                    const T gw = Gauss<T, NPTS>::weight(gp);
-                    T rel[NDIM];
+                for (int axis = 0; axis < NDIM; ++axis) {
+                    T acc[CNT];
+                    int cur[3][P + 1];
+                    bool cur_ex[P > 0 ? P : 1];
+                    bool open = false;
+                    const int cnt0 = axis == 0 ? P : SX;
+                    const int cnt1 = NDIM > 1 ? (axis == 1 ? P : SX) : 1;
+                    const int cnt2 = NDIM > 2 ? (axis == 2 ? P : SX) : 1;
+                    auto flush = [&]() {
 #pragma unroll
-                    for (int d = 0; d < NDIM; ++d) rel[d] = p0[d] + point * step[d];
+                        for (int x = 0; x < cnt0; ++x) {
+                            if (axis == 0 && !cur_ex[x]) continue;
 #pragma unroll
-                    for (int axis = 0; axis < NDIM; ++axis) {
+                            for (int y = 0; y < cnt1; ++y) {
+                                if (NDIM > 1 && axis == 1 && !cur_ex[y]) continue;
+#pragma unroll
+                                for (int z = 0; z < cnt2; ++z) {
+                                    if (NDIM > 2 && axis == 2 && !cur_ex[z]) continue;
+                                    int n[3] = {cur[0][x], NDIM > 1 ? cur[1][y] : 0, NDIM > 2 ? cur[2][z] : 0};
+                                    sink.add(n, axis, acc[(x * cnt1 + y) * cnt2 + z]);
+                                }
+                            }
+                        }
+                    };
+#pragma unroll
+                    for (int gp = 0; gp < NPTS; ++gp) {
+                        const T point = Gauss<T, NPTS>::point(gp);
+                        const T gw = Gauss<T, NPTS>::weight(gp);
                         const T amount = q * gw * step[axis];
                         if (amount == T(0)) continue;
                         int idx[3][P + 1];
@@ -356,33 +382,46 @@ __device__ void spline_path(T q, const T* r0, const T* r1, const Grid<T>& g, con
                         bool ex[P > 0 ? P : 1];
 #pragma unroll
                         for (int d = 0; d < NDIM; ++d) {
+                            const T rel = p0[d] + point * step[d];
                             if (d == axis) {
-                                along_stencil<T, P>(rel[d], g.num[d], g.code[d], idx[d], wt[d], ex);
+                                along_stencil<T, P>(rel, g.num[d], g.code[d], idx[d], wt[d], ex);
                             } else {
-                                const int base = axis_stencil<T, SPLINE, P>(rel[d], g.num[d], g.code[d], wt[d]);
+                                const int base = axis_stencil<T, SPLINE, P>(rel, g.num[d], g.code[d], wt[d]);
 #pragma unroll
                                 for (int s = 0; s <= P; ++s) idx[d][s] = map_node(base + s, g.num[d], g.code[d]);
                             }
                         }
-                        constexpr int SX = P + 1;
-                        const int cnt0 = axis == 0 ? P : SX;
-                        const int cnt1 = NDIM > 1 ? (axis == 1 ? P : SX) : 1;
-                        const int cnt2 = NDIM > 2 ? (axis == 2 ? P : SX) : 1;
-                        for (int x = 0; x < cnt0; ++x) {
-                            if (axis == 0 && !ex[x]) continue;
-                            for (int y = 0; y < cnt1; ++y) {
-                                if (NDIM > 1 && axis == 1 && !ex[y]) continue;
+                        bool same = open;
+#pragma unroll
+                        for (int d = 0; d < NDIM; ++d)
+#pragma unroll
+                            for (int s = 0; s <= P; ++s) same = same && idx[d][s] == cur[d][s];
+#pragma unroll
+                        for (int s = 0; s < (P > 0 ? P : 1); ++s) same = same && ex[s] == cur_ex[s];
+                        if (!same) {
+                            if (open) flush();
+#pragma unroll
+                            for (int d = 0; d < NDIM; ++d)
+#pragma unroll
+                                for (int s = 0; s <= P; ++s) cur[d][s] = idx[d][s];
+#pragma unroll
+                            for (int s = 0; s < (P > 0 ? P : 1); ++s) cur_ex[s] = ex[s];
+                            open = true;
+                        }
+#pragma unroll
+                        for (int x = 0; x < cnt0; ++x)
+#pragma unroll
+                            for (int y = 0; y < cnt1; ++y)
+#pragma unroll
                                 for (int z = 0; z < cnt2; ++z) {
-                                    if (NDIM > 2 && axis == 2 && !ex[z]) continue;
                                     T w = amount * wt[0][x];
                                     if constexpr (NDIM > 1) w = w * wt[1][y];
                                     if constexpr (NDIM > 2) w = w * wt[2][z];
-                                    int n[3] = {idx[0][x], NDIM > 1 ? idx[1][y] : 0, NDIM > 2 ? idx[2][z] : 0};
-                                    sink.add(n, axis, w);
+                                    T& r = acc[(x * cnt1 + y) * cnt2 + z];
+                                    r = same ? r + w : w;
                                 }
-                            }
-                        }
                     }
+                    if (open) flush();
                 }
                 t0 = t1;
             }
