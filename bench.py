@@ -66,6 +66,8 @@ def parse() -> argparse.Namespace:
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-ref-cuda", action="store_true")
     p.add_argument("--no-extras", action="store_true", help="skip the other configurations' measurements")
+    p.add_argument("--serve-requests", type=int, default=1000, help="requests of the serving stream (0: skip)")
+    p.add_argument("--serve-rate", type=float, default=2000.0, help="Poisson arrival rate of the stream, per s")
     return p.parse_args()
 
 
@@ -452,6 +454,15 @@ def run_ours(args, world, rank, local) -> None:
         torch.cuda.empty_cache()
         extras["autograd"] = measure_autograd(device, reps)
         extras["path_deposit"] = measure_paths(device, reps, peak)
+        if args.serve_requests > 0:
+            from mpifield_b200 import serving
+
+            torch.cuda.empty_cache()
+            extras["serving"] = serving.serve_benchmark(args.serve_requests, args.serve_rate, seed=0, device=device)
+            extras["serving"]["what"] = (
+                "mixed stream (Poisson arrivals, ndim 1-3, nodes per axis log-U[32,256], markers log-U[1e3,1e7], "
+                "degree 1-3, gather 3-comp / scatter / path deposit, FP64, 120 GB budget) served with continuous "
+                "batching vs one plain launch per request; latency = completion - arrival")
 
     clock = clocks.summary()
     if rank == 0:

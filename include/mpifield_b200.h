@@ -250,6 +250,68 @@ MPF_API int mpf_permute_rows(void* dst, int64_t dst_stride, const void* src, int
 MPF_API int mpf_unpermute_rows(void* dst, int64_t dst_stride, const void* src, int64_t src_stride,
                                int64_t rows, const int32_t* order, int64_t n, int dtype, void* stream);
 
+/* ------------------------------------------------------------------ serving batches --
+ *
+ * One launch runs many small FP64 gather and scatter requests. The requests sit in a
+ * device table of mpf_batch_request entries; each is cut into tiles of
+ * header->tile_markers markers, and persistent CTAs take tiles from the counter
+ * header->next_tile until header->tiles are done. The last CTA to finish sets the
+ * counter back to zero, so a launch captured once in a CUDA graph replays with new table
+ * contents (the table, the header and their sizes live in device memory the caller
+ * owns). No counterpart in the reference, whose kernels run one call per launch; each
+ * request's arithmetic is that of mpf_gather / mpf_scatter on the same arguments (global
+ * memory, one marker per thread, scatter adds as FP64 atomics).
+ */
+#define MPF_OP_GATHER 0
+#define MPF_OP_SCATTER 1
+
+typedef struct mpf_batch_request {
+    int32_t op, kind, degree, ndim;
+    int32_t ncomp, reserved;
+    int64_t n;
+    int64_t first_tile;          /* tiles of the requests before this one in the table */
+    const double* positions;     /* (ndim, n), rows pos_stride apart */
+    int64_t pos_stride;
+    const double* values;        /* scatter: (ncomp, n), rows val_stride apart */
+    int64_t val_stride;
+    const double* field;         /* gather: extent + (ncomp,) */
+    double* out;                 /* gather: result (ncomp, n) rows out_stride apart; scatter: the field */
+    int64_t out_stride;
+    double lower[3], cell[3], inv[3];
+    int32_t num[3], code[3], ext[3];
+    int32_t pad;
+} mpf_batch_request;
+
+typedef struct mpf_batch_header {
+    int64_t requests;      /* entries of the table */
+    int64_t tiles;         /* tiles of all requests (the last entry's first_tile + its tiles) */
+    int64_t tile_markers;  /* markers per tile */
+    int64_t next_tile;     /* the work counter: zero before a launch, zero again after it */
+    int64_t finished;      /* CTAs done (the last one resets both counters) */
+    int64_t pad[3];
+} mpf_batch_header;
+
+/* sizeof(mpf_batch_request), for bindings that lay the table out themselves. */
+MPF_API int64_t mpf_batch_request_size(void);
+
+/*
+ * Checks one request as mpf_gather / mpf_scatter would and fills *r (host memory) for
+ * the table; first_tile is left for the caller. op MPF_OP_GATHER: values ignored, out is
+ * the result; MPF_OP_SCATTER: field ignored, out is the field added into.
+ */
+MPF_API int mpf_batch_request_init(mpf_batch_request* r, int op, int kind, int degree, int ndim,
+                                   const void* positions, int64_t pos_stride, const void* values,
+                                   int64_t val_stride, int64_t n, const void* field, void* out,
+                                   int64_t out_stride, int ncomp, const double* lower, const double* cell,
+                                   const int32_t* num, const int32_t* code);
+
+/*
+ * The batch launch: table and header in device memory; grid CTAs of block threads
+ * (0: 2 CTAs per SM of 256 threads). Reads the sizes from the header when it runs.
+ */
+MPF_API int mpf_batch_launch(const mpf_batch_request* table, mpf_batch_header* header, int grid, int block,
+                             void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -40,6 +40,26 @@ class Tuning(C.Structure):
                 ("ctas_per_sm", C.c_int32), ("variant", C.c_int32)]
 
 
+class BatchRequest(C.Structure):
+    """``mpf_batch_request``: one request of a serving batch (a device table entry)."""
+
+    _fields_ = [("op", C.c_int32), ("kind", C.c_int32), ("degree", C.c_int32), ("ndim", C.c_int32),
+                ("ncomp", C.c_int32), ("reserved", C.c_int32), ("n", C.c_int64), ("first_tile", C.c_int64),
+                ("positions", C.c_void_p), ("pos_stride", C.c_int64), ("values", C.c_void_p),
+                ("val_stride", C.c_int64), ("field", C.c_void_p), ("out", C.c_void_p), ("out_stride", C.c_int64),
+                ("lower", C.c_double * 3), ("cell", C.c_double * 3), ("inv", C.c_double * 3),
+                ("num", C.c_int32 * 3), ("code", C.c_int32 * 3), ("ext", C.c_int32 * 3), ("pad", C.c_int32)]
+
+
+class BatchHeader(C.Structure):
+    """``mpf_batch_header``: table size, tiles, markers per tile and the work counters."""
+
+    _fields_ = [("requests", C.c_int64), ("tiles", C.c_int64), ("tile_markers", C.c_int64),
+                ("next_tile", C.c_int64), ("finished", C.c_int64), ("pad", C.c_int64 * 3)]
+
+
+OP_GATHER, OP_SCATTER = 0, 1
+
 _P = C.c_void_p
 _I = C.c_int
 _L = C.c_int64
@@ -65,6 +85,9 @@ _SIGNATURES = {
                                   _P], _I),
     "mpf_permute_rows": ([_P, _L, _P, _L, _L, _P, _L, _I, _P], _I),
     "mpf_unpermute_rows": ([_P, _L, _P, _L, _L, _P, _L, _I, _P], _I),
+    "mpf_batch_request_size": ([], _L),
+    "mpf_batch_request_init": ([_P, _I, _I, _I, _I, _P, _L, _P, _L, _L, _P, _P, _L, _I, _P, _P, _P, _P], _I),
+    "mpf_batch_launch": ([_P, _P, _I, _I, _P], _I),
 }
 
 _lock = threading.Lock()

@@ -467,4 +467,55 @@ int mpf_unpermute_rows(void* dst, int64_t dst_stride, const void* src, int64_t s
     return unpermute_rows(dst, dst_stride, src, src_stride, rows, order, n, dtype, static_cast<cudaStream_t>(stream));
 }
 
+int64_t mpf_batch_request_size(void) { return (int64_t)sizeof(mpf_batch_request); }
+
+int mpf_batch_request_init(mpf_batch_request* r, int op, int kind, int degree, int ndim, const void* positions,
+                           int64_t pos_stride, const void* values, int64_t val_stride, int64_t n, const void* field,
+                           void* out, int64_t out_stride, int ncomp, const double* lower, const double* cell,
+                           const int32_t* num, const int32_t* code) {
+    if (!r) return MPF_ERR_ARGUMENT;
+    if (op != MPF_OP_GATHER && op != MPF_OP_SCATTER) return MPF_ERR_ARGUMENT;
+    if (!valid_kind(kind, degree)) return MPF_ERR_ARGUMENT;
+    MPF_TRY(check_grid(kind, degree, ndim, lower, cell, num, code));
+    if (n < 0 || ncomp < 1) return MPF_ERR_ARGUMENT;
+    MPF_TRY(check_rows(positions, pos_stride, n, ndim, MPF_F64));
+    if (!out || !aligned(out, MPF_F64)) return out ? MPF_ERR_ALIGNMENT : MPF_ERR_ARGUMENT;
+    if (op == MPF_OP_GATHER) {
+        if (!field) return MPF_ERR_ARGUMENT;
+        if (!aligned(field, MPF_F64)) return MPF_ERR_ALIGNMENT;
+        MPF_TRY(check_rows(out, out_stride, n, ncomp, MPF_F64));
+    } else {
+        MPF_TRY(check_rows(values, val_stride, n, ncomp, MPF_F64));
+    }
+    std::memset(r, 0, sizeof(*r));
+    r->op = op;
+    r->kind = kind;
+    r->degree = degree;
+    r->ndim = ndim;
+    r->ncomp = ncomp;
+    r->n = n;
+    r->positions = static_cast<const double*>(positions);
+    r->pos_stride = pos_stride;
+    r->values = static_cast<const double*>(values);
+    r->val_stride = val_stride;
+    r->field = static_cast<const double*>(field);
+    r->out = static_cast<double*>(out);
+    r->out_stride = out_stride;
+    const Grid<double> g = make_grid<double>(ndim, degree, lower, cell, num, code);
+    for (int d = 0; d < 3; ++d) {
+        r->lower[d] = g.lower[d];
+        r->cell[d] = g.cell[d];
+        r->inv[d] = g.inv[d];
+        r->num[d] = g.num[d];
+        r->code[d] = g.code[d];
+        r->ext[d] = g.ext[d];
+    }
+    return MPF_OK;
+}
+
+int mpf_batch_launch(const mpf_batch_request* table, mpf_batch_header* header, int grid, int block, void* stream) {
+    if (!table || !header || grid < 0 || block < 0) return MPF_ERR_ARGUMENT;
+    return launch_batch(table, header, grid, block, static_cast<cudaStream_t>(stream));
+}
+
 }  // extern "C"

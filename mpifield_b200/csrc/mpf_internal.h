@@ -114,6 +114,13 @@ int unpermute_rows(void* dst, int64_t ds, const void* src, int64_t ss, int64_t r
                    int64_t n, int dtype, cudaStream_t stream);
 
 int sm_count();
+}  // namespace mpf
+struct mpf_batch_request;
+struct mpf_batch_header;
+namespace mpf {
+// The serving batch launch (mpf_batch.cu).
+int launch_batch(const mpf_batch_request* table, mpf_batch_header* header, int grid, int block,
+                 cudaStream_t stream);
 
 // Counts kernel launches of this library (read by mpf_launch_count).
 void count_launches(int k);

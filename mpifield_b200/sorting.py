@@ -49,13 +49,25 @@ def num_tiles(weighting, geometry, tile) -> int:
     return int(out.value)
 
 
+def sort_workspace_bytes(n: int, ntiles: int) -> int:
+    """Bytes of the sort's workspace for ``n`` markers and ``ntiles`` tiles."""
+    size = C.c_size_t(0)
+    _lib.check(_lib.library().mpf_sort_workspace_bytes(n, ntiles, C.byref(size)), "sort_workspace_bytes")
+    return max(int(size.value), 256)
+
+
+def _empty(shape, dtype, device):
+    return torch.empty(shape, dtype=dtype, device=device)
+
+
 def sort_by_tile(positions: torch.Tensor, weighting, geometry, tile, values: torch.Tensor | None = None,
-                 within: bool = False) -> TileOrder:
+                 within: bool = False, alloc=None) -> TileOrder:
     """Sort markers by cell tile (see the module docstring).
 
     With ``within`` the key continues with the anchor cell inside the tile, so markers of
     one cell end up next to each other (tile-major, then cell-major): the order the
-    gather and scatter kernels run fastest on.
+    gather and scatter kernels run fastest on. ``alloc(shape, dtype)`` supplies the
+    keys, order, tile starts and workspace (default: new tensors on the device).
     """
     kind, degree = _kind_of(weighting)
     lower, cell, num, code, ndim = _lib.geometry_arrays(geometry)
@@ -65,12 +77,11 @@ def sort_by_tile(positions: torch.Tensor, weighting, geometry, tile, values: tor
     n = pos.shape[1]
     ntiles = num_tiles((kind, degree), geometry, tile)
     t = (C.c_int32 * ndim)(*(int(v) for v in tile))
-    size = C.c_size_t(0)
-    _lib.check(_lib.library().mpf_sort_workspace_bytes(n, ntiles, C.byref(size)), "sort_workspace_bytes")
-    workspace = torch.empty(max(int(size.value), 256), dtype=torch.uint8, device=device)
-    keys = torch.empty(n, dtype=torch.int32, device=device)
-    order = torch.empty(n, dtype=torch.int32, device=device)
-    tile_start = torch.empty(ntiles + 2, dtype=torch.int64, device=device)
+    new = alloc or (lambda shape, dt: _empty(shape, dt, device))
+    workspace = new((sort_workspace_bytes(n, ntiles),), torch.uint8)
+    keys = new((n,), torch.int32)
+    order = new((n,), torch.int32)
+    tile_start = new((ntiles + 2,), torch.int64)
     if values is not None:
         vals, vs = _marker_rows(values, values.shape[0] if values.dim() == 2 else 1, "values", dtype)
         vptr, ncomp = vals.data_ptr(), vals.shape[0]
@@ -84,14 +95,17 @@ def sort_by_tile(positions: torch.Tensor, weighting, geometry, tile, values: tor
     return TileOrder(keys, order, tile_start, ntiles)
 
 
-def permute(array: torch.Tensor, order: torch.Tensor) -> torch.Tensor:
-    """``array[:, order]`` for a marker array (rows, N), by the backend's permute kernel."""
+def permute(array: torch.Tensor, order: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:
+    """``array[:, order]`` for a marker array (rows, N), by the backend's permute kernel
+    (into ``out``, a contiguous (rows, N) tensor, when given)."""
     device = _lib.require_cuda(array, order)
     squeeze = array.dim() == 1
     rows = 1 if squeeze else array.shape[0]
     src, ss = _marker_rows(array, rows, "array", array.dtype)
     n = src.shape[1]
-    dst = torch.empty((rows, n), dtype=array.dtype, device=device)
+    dst = torch.empty((rows, n), dtype=array.dtype, device=device) if out is None else out.view(rows, n)
+    if not dst.is_contiguous() or dst.dtype != array.dtype:
+        raise ValueError(f"out must be a contiguous ({rows}, {n}) {array.dtype} tensor")
     order = order.to(torch.int32).contiguous()
     status = _lib.library().mpf_permute_rows(dst.data_ptr(), n, src.data_ptr(), ss, rows, order.data_ptr(), n,
                                             _lib.dtype_code(array.dtype), _lib.stream_of(device))
