@@ -67,6 +67,8 @@ def parse() -> argparse.Namespace:
     p.add_argument("--no-ref-cuda", action="store_true")
     p.add_argument("--no-extras", action="store_true", help="skip the other configurations' measurements")
     p.add_argument("--serve-requests", type=int, default=1000, help="requests of the serving stream (0: skip)")
+    p.add_argument("--paths-only", type=int, default=0, metavar="N",
+                   help="measure only the path deposits, at N paths on 128^3 (a profiling case)")
     p.add_argument("--serve-rate", type=float, default=2000.0, help="Poisson arrival rate of the stream, per s")
     return p.parse_args()
 
@@ -449,6 +451,7 @@ def run_ours(args, world, rank, local) -> None:
     if not args.no_extras and rank == 0 and world == 1 and dtype == torch.float64:
         reps = max(2, args.steps // 2)
         extras["fp32_variant"] = measure_fp32(step, ps, ws, reps)
+        extras["deterministic_scatter"] = measure_deterministic(step, ps, ws, reps)
         extras["plain_2d"] = measure_plain_2d(device, max(10, args.steps))
         del pos, w
         torch.cuda.empty_cache()
@@ -537,14 +540,14 @@ def measure_fp32(step, ps, ws, reps: int) -> dict:
                     "to float32); error relative to max |float64 result|"}
 
 
-def measure_paths(device, reps: int, peak: float) -> dict:
+def measure_paths(device, reps: int, peak: float, n: int = 1 << 25) -> dict:
     """The path deposit: 128^3 periodic, N = 2^25 paths, start uniform, end = start +
     U[-0.9, 0.9] cells per axis, charges U[0.5, 1.5]; WHITNEY and QUADRATIC_EDGES, paths in
     random order and sorted by the start's cell tile; continuity residual
     max |rho(end) - rho(start) - G^T J| with the node deposit of the same degree."""
     import mpifield_b200 as mf
 
-    n, g_n = 1 << 25, 128
+    g_n = 128
     g = torch.Generator(device=device).manual_seed(7)
     start = torch.rand((3, n), generator=g, device=device, dtype=torch.float64)
     end = start + (torch.rand((3, n), generator=g, device=device, dtype=torch.float64) * 1.8 - 0.9) / g_n
@@ -616,6 +619,29 @@ def measure_autograd(device, reps: int) -> dict:
         ms = _event_ms(go, reps)
         out[name] = {"value": n / (ms / 1000.0), "ms_per_step": ms}
     return out
+
+
+def measure_deterministic(step, ps, ws, reps: int) -> dict:
+    """The bit-reproducible scatter on the headline store: time, identical bits on a repeat,
+    and its largest difference from the FP64 atomic scatter (relative to max |density|)."""
+    from mpifield_b200 import _lib
+    from mpifield_b200.kernels import scatter_deterministic
+
+    density = torch.zeros_like(step.density)
+    workspace = torch.empty(16 * density.numel() + 4096, dtype=torch.uint8, device=ps.device)
+
+    def go():
+        density.zero_()
+        scatter_deterministic(_lib.QUADRATIC, 2, ps, ws, density, step.geom, workspace)
+
+    ms = _event_ms(go, reps)
+    first = density.clone()
+    go()
+    same = bool(torch.equal(first.view(torch.int64), density.view(torch.int64)))
+    step.gather_scatter(ps, ws)
+    diff = float((density - step.density).abs().max() / step.density.abs().max())
+    return {"value": ps.shape[1] / (ms / 1000.0), "unit": "markers/s", "ms": ms, "bitwise_repeatable": same,
+            "max_rel_diff_vs_atomic_scatter": diff}
 
 
 def measure_plain_2d(device, reps: int) -> dict:
@@ -691,6 +717,13 @@ def main() -> None:
     GRID = args.grid
     world, rank, local = dist_setup(args)
     try:
+        if args.paths_only > 0:
+            device = torch.device("cuda", local)
+            torch.cuda.set_device(device)
+            if rank == 0:
+                peak, _ = read_peak()
+                print(json.dumps({"path_deposit": measure_paths(device, max(1, args.steps), peak, args.paths_only)}))
+            return
         if args.impl == "reference":
             run_reference(args, world, rank)
         else:

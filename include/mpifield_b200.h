@@ -118,6 +118,25 @@ MPF_API int mpf_scatter(int kind, int degree, int ndim, const void* positions, i
                 const double* lower, const double* cell, const int32_t* num, const int32_t* code,
                 int dtype, const mpf_tuning* tuning, void* stream);
 
+/* Bytes of the workspace of mpf_scatter_deterministic for a field of `entries` values
+ * (the product of its extent and ncomp). */
+MPF_API int mpf_scatter_deterministic_workspace_bytes(int64_t entries, size_t* bytes);
+
+/*
+ * The bit-reproducible scatter (FP64 only): field(k, c) += sum_i W_k(x_i) values(c, i)
+ * as mpf_scatter computes it, every contribution summed as a pair of 64-bit fixed-point
+ * integers (integer adds are associative), so the result has the same bits for every run,
+ * launch shape and order of the markers; it differs from the FP64 atomic scatter by
+ * rounding only (the fixed-point quantum is about 1e-19 of N max |values|). The values
+ * must be finite. workspace: mpf_scatter_deterministic_workspace_bytes bytes, 16-byte
+ * aligned, owned by the caller. No counterpart in the reference, whose scatters add
+ * floating-point atomics in arrival order.
+ */
+MPF_API int mpf_scatter_deterministic(int kind, int degree, int ndim, const void* positions, int64_t pos_stride,
+                                      const void* values, int64_t val_stride, int64_t n, void* field,
+                                      int64_t ncomp, const double* lower, const double* cell, const int32_t* num,
+                                      const int32_t* code, void* workspace, size_t workspace_bytes, void* stream);
+
 /*
  * Position gradient of a gather contracted with a cotangent, for reverse mode:
  * grad(d, i) = sum_c cot(c, i) d/dx_d sum_k W_k(x_i) field(k, c), overwriting grad

@@ -235,6 +235,37 @@ int mpf_scatter(int kind, int degree, int ndim, const void* positions, int64_t p
     return launch_scatter<float>(kind, degree, ndim, a, t, s);
 }
 
+int mpf_scatter_deterministic_workspace_bytes(int64_t entries, size_t* bytes) {
+    if (entries < 0 || !bytes) return MPF_ERR_ARGUMENT;
+    *bytes = det_workspace_bytes(entries);
+    return MPF_OK;
+}
+
+int mpf_scatter_deterministic(int kind, int degree, int ndim, const void* positions, int64_t pos_stride,
+                              const void* values, int64_t val_stride, int64_t n, void* field, int64_t ncomp,
+                              const double* lower, const double* cell, const int32_t* num, const int32_t* code,
+                              void* workspace, size_t workspace_bytes, void* stream) {
+    if (!valid_kind(kind, degree)) return MPF_ERR_ARGUMENT;
+    MPF_TRY(check_grid(kind, degree, ndim, lower, cell, num, code));
+    if (n < 0 || ncomp < 1 || ncomp > (1 << 20)) return MPF_ERR_ARGUMENT;
+    MPF_TRY(check_rows(positions, pos_stride, n, ndim, MPF_F64));
+    MPF_TRY(check_rows(values, val_stride, n, (int)ncomp, MPF_F64));
+    if (n == 0) return MPF_OK;
+    if (!field) return MPF_ERR_ARGUMENT;
+    if (!aligned(field, MPF_F64)) return MPF_ERR_ALIGNMENT;
+    const Grid<double> g = make_grid<double>(ndim, degree, lower, cell, num, code);
+    int64_t entries = ncomp;
+    for (int d = 0; d < ndim; ++d) entries *= g.ext[d];
+    if (!workspace) return MPF_ERR_ARGUMENT;
+    if (reinterpret_cast<uintptr_t>(workspace) % 16 != 0) return MPF_ERR_ALIGNMENT;
+    if (workspace_bytes < det_workspace_bytes(entries)) return MPF_ERR_WORKSPACE;
+    NodeArgs<double> a = node_args<double>(ndim, degree, lower, cell, num, code);
+    a.pos = (const double*)positions; a.pos_stride = pos_stride;
+    a.values = (const double*)values; a.val_stride = val_stride;
+    a.field_out = (double*)field; a.n = n; a.ncomp = (int)ncomp;
+    return launch_scatter_deterministic(kind, degree, ndim, a, entries, workspace, static_cast<cudaStream_t>(stream));
+}
+
 int mpf_gather_grad(int kind, int degree, int ndim, const void* positions, int64_t pos_stride, int64_t n,
                     const void* field, int64_t ncomp, const void* cotangent, int64_t cot_stride, void* grad,
                     int64_t grad_stride, const double* lower, const double* cell, const int32_t* num,
@@ -273,7 +304,7 @@ int mpf_deposit_paths(int kind, int degree, int ndim, const void* start, int64_t
                       int64_t end_stride, const void* charges, int64_t n, void* edges, const double* lower,
                       const double* cell, const int32_t* num, const int32_t* code, int dtype,
                       const mpf_tuning* tuning, void* stream) {
-    (void)tuning;
+    const Tuning t = tuning_of(tuning);
     if (!valid_edge_kind(kind, degree) || (dtype != MPF_F64 && dtype != MPF_F32)) return MPF_ERR_ARGUMENT;
     MPF_TRY(check_grid(kind == MPF_LINEAR ? MPF_LINEAR : MPF_SPLINE, degree, ndim, lower, cell, num, code));
     if (n < 0) return MPF_ERR_ARGUMENT;
@@ -292,7 +323,7 @@ int mpf_deposit_paths(int kind, int degree, int ndim, const void* start, int64_t
         a.start = (const double*)start; a.start_stride = start_stride;
         a.end = (const double*)end; a.end_stride = end_stride;
         a.charges = (const double*)charges; a.edges_out = (double*)edges; a.n = n;
-        return launch_deposit_paths<double>(kind, degree, ndim, a, s);
+        return launch_deposit_paths<double>(kind, degree, ndim, a, t, s);
     }
     PathArgs<float> a;
     std::memset(&a, 0, sizeof(a));
@@ -300,7 +331,7 @@ int mpf_deposit_paths(int kind, int degree, int ndim, const void* start, int64_t
     a.start = (const float*)start; a.start_stride = start_stride;
     a.end = (const float*)end; a.end_stride = end_stride;
     a.charges = (const float*)charges; a.edges_out = (float*)edges; a.n = n;
-    return launch_deposit_paths<float>(kind, degree, ndim, a, s);
+    return launch_deposit_paths<float>(kind, degree, ndim, a, t, s);
 }
 
 int mpf_gather_edges(int kind, int degree, int ndim, const void* positions, int64_t pos_stride, int64_t n,

@@ -72,6 +72,8 @@ template <typename T> struct PathArgs {
     T* result;
     int64_t res_stride;
     int64_t n;
+    int capacity;          // deposit: shared-memory edge box, elements of T (0: global atomics only)
+    int paths_per_thread;  // deposit: paths a thread takes per chunk
 };
 
 // The cell-tile keys of the markers.
@@ -91,7 +93,7 @@ template <typename T> struct KeyArgs {
 };
 
 template <typename T>
-int launch_deposit_paths(int kind, int degree, int ndim, const PathArgs<T>& a, cudaStream_t stream);
+int launch_deposit_paths(int kind, int degree, int ndim, PathArgs<T> a, const Tuning& t, cudaStream_t stream);
 template <typename T>
 int launch_gather_edges(int kind, int degree, int ndim, const PathArgs<T>& a, cudaStream_t stream);
 
@@ -118,6 +120,10 @@ int sm_count();
 struct mpf_batch_request;
 struct mpf_batch_header;
 namespace mpf {
+// The bit-reproducible scatter (mpf_deterministic.cu).
+size_t det_workspace_bytes(int64_t entries);
+int launch_scatter_deterministic(int kind, int degree, int ndim, const NodeArgs<double>& a, int64_t entries,
+                                 void* workspace, cudaStream_t s);
 // The serving batch launch (mpf_batch.cu).
 int launch_batch(const mpf_batch_request* table, mpf_batch_header* header, int grid, int block,
                  cudaStream_t stream);

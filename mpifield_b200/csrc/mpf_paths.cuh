@@ -23,6 +23,7 @@
 // same ascending order, so the pieces are the same.
 #pragma once
 #include "mpf_internal.h"
+#include "mpf_nodes.cuh"
 #include "mpf_stencil.cuh"
 
 namespace mpf {
@@ -144,19 +145,11 @@ __device__ __forceinline__ int floor_to_int(float x) {
     return whole;
 }
 
-// The P edges along an axis around rel: their (mapped) first nodes, weights
-// B_{P-1}(rel - k - 1/2) and whether each exists (spline_edges.cuh:22-65).
+// The P edges along a periodic or bounded axis around rel: their (mapped) first nodes,
+// whether each exists, and the offset t of rel - 1/2 from the middle of the degree P - 1
+// stencil (the weights are uniform_weights<P - 1>(t)).
 template <typename T, int P>
-__device__ __forceinline__ void along_stencil(T rel, int num, int code, int* edge, T* weight, bool* exists) {
-    if (code == CLAMPED) {
-        const int cell = clamped_cell<T, P, true>(rel, num, weight);
-#pragma unroll
-        for (int a = 0; a < P; ++a) {
-            edge[a] = cell + a;
-            exists[a] = true;
-        }
-        return;
-    }
+__device__ __forceinline__ void along_frame(T rel, int num, int code, int* edge, bool* exists, T& t) {
     constexpr int LOWER = P - 1;
     if (code == PERIODIC && !(rel >= T(0) && rel < T(num))) rel = wrap_period(rel, num);
     const T shifted = rel - T(0.5);
@@ -168,7 +161,7 @@ __device__ __forceinline__ void along_stencil(T rel, int num, int code, int* edg
         middle = floor_to_int(shifted);
     }
     middle = clampi(middle, -2, num + 1);
-    uniform_weights<T, LOWER>(shifted - T(middle), weight);
+    t = shifted - T(middle);
     const int first = middle - LOWER / 2;
 #pragma unroll
     for (int a = 0; a < P; ++a) {
@@ -184,6 +177,24 @@ __device__ __forceinline__ void along_stencil(T rel, int num, int code, int* edg
             exists[a] = true;
         }
     }
+}
+
+// The P edges along an axis around rel: their (mapped) first nodes, weights
+// B_{P-1}(rel - k - 1/2) and whether each exists (spline_edges.cuh:22-65).
+template <typename T, int P>
+__device__ __forceinline__ void along_stencil(T rel, int num, int code, int* edge, T* weight, bool* exists) {
+    if (code == CLAMPED) {
+        const int cell = clamped_cell<T, P, true>(rel, num, weight);
+#pragma unroll
+        for (int a = 0; a < P; ++a) {
+            edge[a] = cell + a;
+            exists[a] = true;
+        }
+        return;
+    }
+    T t;
+    along_frame<T, P>(rel, num, code, edge, exists, t);
+    uniform_weights<T, P - 1>(t, weight);
 }
 
 // Gauss-Legendre points and weights on [0, 1] for COUNT = 1..5 points: the values of
@@ -294,6 +305,9 @@ __device__ void spline_path(T q, const T* r0, const T* r1, const Grid<T>& g, con
         const T span = r1[d] > r0[d] ? r1[d] - r0[d] : r0[d] - r1[d];
         if (span > extent) extent = span;
     }
+    bool clamped = false;
+#pragma unroll
+    for (int d = 0; d < NDIM; ++d) clamped = clamped || g.code[d] == CLAMPED;
     int stretches = trunc_int<T>(extent / T(4)) + 1;
     if (stretches > kMaxPathSteps || stretches < 1) stretches = kMaxPathSteps;
     for (int st = 0; st < stretches; ++st) {
@@ -340,94 +354,403 @@ __device__ void spline_path(T q, const T* r0, const T* r1, const Grid<T>& g, con
                     p0[d] = begin;
                     step[d] = finish - begin;
                 }
-                // The Gauss points of a piece lie in one knot interval on every axis, so
-                // they share the edges of their stencils: their contributions are summed
-                // in registers and added once per piece and axis (a point whose stencil
-                // differs -- rounding at a cut -- closes the sum and opens a new one).
-                constexpr int SX = P + 1;
-                constexpr int CNT = P * (NDIM > 1 ? SX : 1) * (NDIM > 2 ? SX : 1);
+                if (!clamped) {
+                    // The Gauss points of a piece lie in one knot interval on every axis:
+                    // the nodes, the edges and their existence are those of the piece's
+                    // midpoint, and a point's weights are the stencil polynomials at the
+                    // midpoint's offset plus (point - 1/2) times the step. The contributions
+                    // of the points are summed in registers, one atomic per edge and axis.
+                    int sidx[3][P + 1], aidx[3][P > 0 ? P : 1];
+                    bool aex[3][P > 0 ? P : 1];
+                    T st[3], at[3];
 #pragma unroll
-                for (int axis = 0; axis < NDIM; ++axis) {
-                    T acc[CNT];
-                    int cur[3][P + 1];
-                    bool cur_ex[P > 0 ? P : 1];
-                    bool open = false;
-                    const int cnt0 = axis == 0 ? P : SX;
-                    const int cnt1 = NDIM > 1 ? (axis == 1 ? P : SX) : 1;
-                    const int cnt2 = NDIM > 2 ? (axis == 2 ? P : SX) : 1;
-                    auto flush = [&]() {
+                    for (int d = 0; d < NDIM; ++d) {
+                        const T mid = p0[d] + T(0.5) * step[d];
+                        const int first = spline_frame<T, P>(mid, g.num[d], g.code[d], st[d]);
+#pragma unroll
+                        for (int s = 0; s <= P; ++s) sidx[d][s] = map_node(first + s, g.num[d], g.code[d]);
+                        along_frame<T, P>(mid, g.num[d], g.code[d], aidx[d], aex[d], at[d]);
+                    }
+                    constexpr int SX = P + 1;
+#pragma unroll
+                    for (int axis = 0; axis < NDIM; ++axis) {
+                        if (q * step[axis] == T(0)) continue;
+                        const int cnt0 = axis == 0 ? P : SX;
+                        const int cnt1 = NDIM > 1 ? (axis == 1 ? P : SX) : 1;
+                        const int cnt2 = NDIM > 2 ? (axis == 2 ? P : SX) : 1;
+                        T acc[P * (NDIM > 1 ? SX : 1) * (NDIM > 2 ? SX : 1)];
+#pragma unroll
+                        for (int k = 0; k < cnt0 * cnt1 * cnt2; ++k) acc[k] = T(0);
+#pragma unroll
+                        for (int gp = 0; gp < NPTS; ++gp) {
+                            const T off = Gauss<T, NPTS>::point(gp) - T(0.5);
+                            const T amount = q * Gauss<T, NPTS>::weight(gp) * step[axis];
+                            T wt[3][P + 1];
+#pragma unroll
+                            for (int d = 0; d < NDIM; ++d) {
+                                if (d == axis) uniform_weights<T, P - 1>(at[d] + off * step[d], wt[d]);
+                                else uniform_weights<T, P>(st[d] + off * step[d], wt[d]);
+                            }
+#pragma unroll
+                            for (int x = 0; x < cnt0; ++x)
+#pragma unroll
+                                for (int y = 0; y < cnt1; ++y) {
+                                    T wxy = amount * wt[0][x];
+                                    if constexpr (NDIM > 1) wxy = wxy * wt[1][y];
+#pragma unroll
+                                    for (int z = 0; z < cnt2; ++z) {
+                                        T& r = acc[(x * cnt1 + y) * cnt2 + z];
+                                        if constexpr (NDIM > 2) r = fma(wxy, wt[2][z], r);
+                                        else r = r + wxy;
+                                    }
+                                }
+                        }
 #pragma unroll
                         for (int x = 0; x < cnt0; ++x) {
-                            if (axis == 0 && !cur_ex[x]) continue;
+                            if (axis == 0 && !aex[0][x]) continue;
 #pragma unroll
                             for (int y = 0; y < cnt1; ++y) {
-                                if (NDIM > 1 && axis == 1 && !cur_ex[y]) continue;
+                                if (NDIM > 1 && axis == 1 && !aex[1][y]) continue;
 #pragma unroll
                                 for (int z = 0; z < cnt2; ++z) {
-                                    if (NDIM > 2 && axis == 2 && !cur_ex[z]) continue;
-                                    int n[3] = {cur[0][x], NDIM > 1 ? cur[1][y] : 0, NDIM > 2 ? cur[2][z] : 0};
+                                    if (NDIM > 2 && axis == 2 && !aex[2][z]) continue;
+                                    int n[3];
+                                    n[0] = axis == 0 ? aidx[0][x] : sidx[0][x];
+                                    n[1] = NDIM > 1 ? (axis == 1 ? aidx[1][y] : sidx[1][y]) : 0;
+                                    n[2] = NDIM > 2 ? (axis == 2 ? aidx[2][z] : sidx[2][z]) : 0;
                                     sink.add(n, axis, acc[(x * cnt1 + y) * cnt2 + z]);
                                 }
                             }
                         }
-                    };
-#pragma unroll
-                    for (int gp = 0; gp < NPTS; ++gp) {
-                        const T point = Gauss<T, NPTS>::point(gp);
-                        const T gw = Gauss<T, NPTS>::weight(gp);
-                        const T amount = q * gw * step[axis];
-                        if (amount == T(0)) continue;
-                        int idx[3][P + 1];
-                        T wt[3][P + 1];
-                        bool ex[P > 0 ? P : 1];
-#pragma unroll
-                        for (int d = 0; d < NDIM; ++d) {
-                            const T rel = p0[d] + point * step[d];
-                            if (d == axis) {
-                                along_stencil<T, P>(rel, g.num[d], g.code[d], idx[d], wt[d], ex);
-                            } else {
-                                const int base = axis_stencil<T, SPLINE, P>(rel, g.num[d], g.code[d], wt[d]);
-#pragma unroll
-                                for (int s = 0; s <= P; ++s) idx[d][s] = map_node(base + s, g.num[d], g.code[d]);
-                            }
-                        }
-                        bool same = open;
-#pragma unroll
-                        for (int d = 0; d < NDIM; ++d)
-#pragma unroll
-                            for (int s = 0; s <= P; ++s) same = same && idx[d][s] == cur[d][s];
-#pragma unroll
-                        for (int s = 0; s < (P > 0 ? P : 1); ++s) same = same && ex[s] == cur_ex[s];
-                        if (!same) {
-                            if (open) flush();
-#pragma unroll
-                            for (int d = 0; d < NDIM; ++d)
-#pragma unroll
-                                for (int s = 0; s <= P; ++s) cur[d][s] = idx[d][s];
-#pragma unroll
-                            for (int s = 0; s < (P > 0 ? P : 1); ++s) cur_ex[s] = ex[s];
-                            open = true;
-                        }
-#pragma unroll
-                        for (int x = 0; x < cnt0; ++x)
-#pragma unroll
-                            for (int y = 0; y < cnt1; ++y)
-#pragma unroll
-                                for (int z = 0; z < cnt2; ++z) {
-                                    T w = amount * wt[0][x];
-                                    if constexpr (NDIM > 1) w = w * wt[1][y];
-                                    if constexpr (NDIM > 2) w = w * wt[2][z];
-                                    T& r = acc[(x * cnt1 + y) * cnt2 + z];
-                                    r = same ? r + w : w;
-                                }
                     }
-                    if (open) flush();
+                } else {
+                    // The Gauss points of a piece lie in one knot interval on every axis, so
+                    // they share the edges of their stencils: their contributions are summed
+                    // in registers and added once per piece and axis (a point whose stencil
+                    // differs -- rounding at a cut -- closes the sum and opens a new one).
+                    constexpr int SX = P + 1;
+                    constexpr int CNT = P * (NDIM > 1 ? SX : 1) * (NDIM > 2 ? SX : 1);
+    #pragma unroll
+                    for (int axis = 0; axis < NDIM; ++axis) {
+                        T acc[CNT];
+                        int cur[3][P + 1];
+                        bool cur_ex[P > 0 ? P : 1];
+                        bool open = false;
+                        const int cnt0 = axis == 0 ? P : SX;
+                        const int cnt1 = NDIM > 1 ? (axis == 1 ? P : SX) : 1;
+                        const int cnt2 = NDIM > 2 ? (axis == 2 ? P : SX) : 1;
+                        auto flush = [&]() {
+    #pragma unroll
+                            for (int x = 0; x < cnt0; ++x) {
+                                if (axis == 0 && !cur_ex[x]) continue;
+    #pragma unroll
+                                for (int y = 0; y < cnt1; ++y) {
+                                    if (NDIM > 1 && axis == 1 && !cur_ex[y]) continue;
+    #pragma unroll
+                                    for (int z = 0; z < cnt2; ++z) {
+                                        if (NDIM > 2 && axis == 2 && !cur_ex[z]) continue;
+                                        int n[3] = {cur[0][x], NDIM > 1 ? cur[1][y] : 0, NDIM > 2 ? cur[2][z] : 0};
+                                        sink.add(n, axis, acc[(x * cnt1 + y) * cnt2 + z]);
+                                    }
+                                }
+                            }
+                        };
+    #pragma unroll
+                        for (int gp = 0; gp < NPTS; ++gp) {
+                            const T point = Gauss<T, NPTS>::point(gp);
+                            const T gw = Gauss<T, NPTS>::weight(gp);
+                            const T amount = q * gw * step[axis];
+                            if (amount == T(0)) continue;
+                            int idx[3][P + 1];
+                            T wt[3][P + 1];
+                            bool ex[P > 0 ? P : 1];
+    #pragma unroll
+                            for (int d = 0; d < NDIM; ++d) {
+                                const T rel = p0[d] + point * step[d];
+                                if (d == axis) {
+                                    along_stencil<T, P>(rel, g.num[d], g.code[d], idx[d], wt[d], ex);
+                                } else {
+                                    const int base = axis_stencil<T, SPLINE, P>(rel, g.num[d], g.code[d], wt[d]);
+    #pragma unroll
+                                    for (int s = 0; s <= P; ++s) idx[d][s] = map_node(base + s, g.num[d], g.code[d]);
+                                }
+                            }
+                            bool same = open;
+    #pragma unroll
+                            for (int d = 0; d < NDIM; ++d)
+    #pragma unroll
+                                for (int s = 0; s <= P; ++s) same = same && idx[d][s] == cur[d][s];
+    #pragma unroll
+                            for (int s = 0; s < (P > 0 ? P : 1); ++s) same = same && ex[s] == cur_ex[s];
+                            if (!same) {
+                                if (open) flush();
+    #pragma unroll
+                                for (int d = 0; d < NDIM; ++d)
+    #pragma unroll
+                                    for (int s = 0; s <= P; ++s) cur[d][s] = idx[d][s];
+    #pragma unroll
+                                for (int s = 0; s < (P > 0 ? P : 1); ++s) cur_ex[s] = ex[s];
+                                open = true;
+                            }
+    #pragma unroll
+                            for (int x = 0; x < cnt0; ++x)
+    #pragma unroll
+                                for (int y = 0; y < cnt1; ++y)
+    #pragma unroll
+                                    for (int z = 0; z < cnt2; ++z) {
+                                        T w = amount * wt[0][x];
+                                        if constexpr (NDIM > 1) w = w * wt[1][y];
+                                        if constexpr (NDIM > 2) w = w * wt[2][z];
+                                        T& r = acc[(x * cnt1 + y) * cnt2 + z];
+                                        r = same ? r + w : w;
+                                    }
+                        }
+                        if (open) flush();
+                    }
                 }
                 t0 = t1;
             }
             if (which < 0) break;
         }
     }
+}
+
+
+
+// The cell coordinates of path i's ends; false for a path whose ends are not finite
+// (it deposits nothing: src/mpifield/edges.py:87).
+template <typename T, int NDIM, bool WHITNEY>
+__device__ __forceinline__ bool path_cells(const PathArgs<T>& a, int64_t i, T* r0, T* r1) {
+    bool finite = true;
+#pragma unroll
+    for (int d = 0; d < NDIM; ++d) {
+        const T s = a.start[d * a.start_stride + i];
+        const T e = a.end[d * a.end_stride + i];
+        r0[d] = (s - a.g.lower[d]) / a.g.cell[d];
+        r1[d] = (e - a.g.lower[d]) / a.g.cell[d];
+        if constexpr (WHITNEY) {
+            const T big = sizeof(T) == 8 ? T(1e300) : T(3e38);
+            if (!(r0[d] > -big && r0[d] < big && r1[d] > -big && r1[d] < big)) finite = false;
+        } else {
+            if (!(s - s == T(0)) || !(e - e == T(0))) finite = false;
+        }
+    }
+    return finite;
+}
+
+// edges += the box of a sink (its non-zero entries), with global atomics.
+template <typename T, int NDIM, typename Sink, typename G>
+__device__ __forceinline__ void flush_edge_box(const T* tile, T* edges, const Sink& sink, const G& g) {
+    int vol = NDIM;
+#pragma unroll
+    for (int d = 0; d < NDIM; ++d) vol *= sink.ex[d];
+    for (int k = threadIdx.x; k < vol; k += blockDim.x) {
+        const T v = tile[k];
+        if (v == T(0)) continue;
+        const int axis = k % NDIM;
+        int rest = k / NDIM;
+        int node[3];
+#pragma unroll
+        for (int d = NDIM - 1; d >= 0; --d) {
+            const int r = rest % sink.ex[d];
+            rest /= sink.ex[d];
+            int n = sink.lo[d] + r;
+            if (sink.periodic[d] && n >= g.num[d]) n -= g.num[d];
+            node[d] = n;
+        }
+        int64_t gi = node[0];
+#pragma unroll
+        for (int d = 1; d < NDIM; ++d) gi = gi * g.ext[d] + node[d];
+        atomicAdd(edges + gi * NDIM + axis, v);
+    }
+}
+
+// Adds v to edge (node per axis, axis) in the chunk's box of edges in shared memory when
+// the node lies in it, else with a global atomic. On a periodic axis the box is an arc of
+// the period: the node is inside when (node - lo) mod num < ex.
+template <typename T, int NDIM> struct BoxEdgeSink {
+    T* tile;
+    T* edges;
+    int lo[3], ex[3], num[3], ext[3];
+    bool periodic[3];
+    bool staged;
+    __device__ __forceinline__ void add(const int* node, int axis, T v) const {
+        if (staged) {
+            int k = 0;
+            bool inside = true;
+#pragma unroll
+            for (int d = 0; d < NDIM; ++d) {
+                int r = node[d] - lo[d];
+                if (periodic[d] && r < 0) r += num[d];
+                inside = inside && (unsigned)r < (unsigned)ex[d];
+                k = k * ex[d] + r;
+            }
+            if (inside) {
+                atomicAdd(tile + k * NDIM + axis, v);
+                return;
+            }
+        }
+        int64_t g = node[0];
+#pragma unroll
+        for (int d = 1; d < NDIM; ++d) g = g * ext[d] + node[d];
+        atomicAdd(edges + g * NDIM + axis, v);
+    }
+};
+
+// The range of cells whose edges a path can touch along one axis (pre-mapping, with a
+// margin for the rounding of the kernel's own cell coordinates).
+template <typename T, int P>
+__device__ __forceinline__ void path_reach(T r0, T r1, int& first, int& last) {
+    constexpr int REACH = P + 1;
+    const T lo = r0 < r1 ? r0 : r1;
+    const T hi = r0 < r1 ? r1 : r0;
+    const T cap = T(1 << 29);
+    first = floor_to_int(lo > -cap ? lo : -cap) - REACH;
+    last = floor_to_int(hi < cap ? hi : cap) + REACH;
+}
+
+// The path deposit on markers sorted by cell tile. A CTA takes a contiguous range of
+// chunks of blockDim x paths_per_thread paths. Pass 1 reduces the chunk's reach to a box
+// per axis (on a periodic axis in whichever of two frames, the plain one or one shifted
+// by half a period, gives the shorter span, so a chunk across the seam stays compact);
+// when the box's edges fit the shared memory, pass 2 deposits every path of the chunk
+// into it (shared-memory atomic adds) and the box is added to the edge field once, with
+// global atomics, when the next chunk needs another box. Otherwise the chunk's paths add
+// to global memory as in deposit_paths_kernel. The arithmetic of each path is that of
+// whitney_path / spline_path.
+template <typename T, int NDIM, int P, bool WHITNEY>
+__global__ void __launch_bounds__(256) deposit_paths_tiled_kernel(const PathArgs<T> a) {
+    __shared__ int s_lo[3], s_hi[3], s_lo2[3], s_hi2[3];
+    T* tile = reinterpret_cast<T*>(mpf_dynamic_smem);
+    BoxEdgeSink<T, NDIM> sink;
+    sink.tile = tile;
+    sink.edges = a.edges_out;
+    int half[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        sink.num[d] = a.g.num[d];
+        sink.ext[d] = a.g.ext[d];
+        sink.periodic[d] = a.g.code[d] == PERIODIC;
+        sink.lo[d] = 0;
+        sink.ex[d] = 1;
+        half[d] = a.g.num[d] / 2;
+    }
+    sink.staged = false;
+    bool have_box = false;
+    const int ppt = a.paths_per_thread;
+    const int64_t CH = (int64_t)blockDim.x * ppt;
+    const int64_t nchunks = (a.n + CH - 1) / CH;
+    int64_t c_first, c_last;
+    chunk_range(nchunks, c_first, c_last);
+    for (int64_t ci = c_first; ci < c_last; ++ci) {
+        const int64_t first = ci * CH;
+        // pass 1: the reach of the chunk's live paths, in both frames
+        int lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
+        int lo2[3] = {INT_MAX, INT_MAX, INT_MAX}, hi2[3] = {INT_MIN, INT_MIN, INT_MIN};
+        for (int m = 0; m < ppt; ++m) {
+            const int64_t i = first + (int64_t)m * blockDim.x + threadIdx.x;
+            if (i >= a.n) continue;
+            const T q = a.charges[i];
+            if (q == T(0)) continue;
+            T r0[NDIM], r1[NDIM];
+            if (!path_cells<T, NDIM, WHITNEY>(a, i, r0, r1)) continue;
+#pragma unroll
+            for (int d = 0; d < NDIM; ++d) {
+                int f, l;
+                path_reach<T, P>(r0[d], r1[d], f, l);
+                if (a.g.code[d] == PERIODIC) {
+                    const int span = l - f;
+                    const int s0 = wrap_index(f, a.g.num[d]);
+                    const int s1 = wrap_index(f + half[d], a.g.num[d]) + a.g.num[d] - half[d];
+                    lo[d] = min(lo[d], s0);
+                    hi[d] = max(hi[d], s0 + span);
+                    lo2[d] = min(lo2[d], s1);
+                    hi2[d] = max(hi2[d], s1 + span);
+                } else {
+                    lo[d] = min(lo[d], clampi(f, 0, a.g.ext[d] - 1));
+                    hi[d] = max(hi[d], clampi(l, 0, a.g.ext[d] - 1));
+                }
+            }
+        }
+        bool staged = false;
+        if (a.capacity > 0) {
+            if (threadIdx.x < 3) {
+                s_lo[threadIdx.x] = INT_MAX;
+                s_hi[threadIdx.x] = INT_MIN;
+                s_lo2[threadIdx.x] = INT_MAX;
+                s_hi2[threadIdx.x] = INT_MIN;
+            }
+            __syncthreads();
+            block_box<NDIM>(lo, hi, s_lo, s_hi);
+            block_box<NDIM>(lo2, hi2, s_lo2, s_hi2);
+            __syncthreads();
+            int nlo[3] = {0, 0, 0}, nex[3] = {1, 1, 1};
+            bool empty = false;
+            int64_t vol = NDIM;
+#pragma unroll
+            for (int d = 0; d < NDIM; ++d) {
+                int l = s_lo[d], h = s_hi[d];
+                if (h < l) empty = true;
+                if (a.g.code[d] == PERIODIC && s_hi2[d] - s_lo2[d] < h - l) {
+                    l = s_lo2[d];
+                    h = s_hi2[d];
+                }
+                if (a.g.code[d] == PERIODIC) {
+                    nlo[d] = wrap_index(l, a.g.num[d]);
+                    nex[d] = min(h - l + 1, a.g.num[d]);
+                } else {
+                    nlo[d] = l;
+                    nex[d] = h - l + 1;
+                }
+                vol *= nex[d] > 0 ? nex[d] : 1;
+            }
+            if (empty) {  // no live path in the chunk
+                __syncthreads();
+                continue;
+            }
+            bool holds = have_box;
+#pragma unroll
+            for (int d = 0; d < NDIM; ++d) {
+                int r = nlo[d] - sink.lo[d];
+                if (sink.periodic[d] && r < 0) r += a.g.num[d];
+                holds = holds && r >= 0 && r + nex[d] <= sink.ex[d];
+            }
+            if (holds) {
+                staged = true;
+            } else if (vol <= (int64_t)a.capacity) {
+                if (have_box) flush_edge_box<T, NDIM>(tile, a.edges_out, sink, a.g);
+                __syncthreads();
+                for (int k = threadIdx.x; k < (int)vol; k += blockDim.x) tile[k] = T(0);
+#pragma unroll
+                for (int d = 0; d < NDIM; ++d) {
+                    sink.lo[d] = nlo[d];
+                    sink.ex[d] = nex[d];
+                }
+                __syncthreads();
+                have_box = true;
+                staged = true;
+            }
+        }
+        sink.staged = staged;
+        // pass 2: the paths, into the box where it holds them. Lane l of warp w takes the
+        // paths l * (warps * ppt) + w * ppt + m of the chunk: the lanes of a warp are
+        // warps * ppt paths apart, in different cells of a sorted store, so that their
+        // shared-memory adds of one instruction land on different nodes.
+        const int warps = blockDim.x >> 5;
+        const int64_t base = first + (int64_t)(threadIdx.x & 31) * warps * ppt + (int64_t)(threadIdx.x >> 5) * ppt;
+        for (int m = 0; m < ppt; ++m) {
+            const int64_t i = base + m;
+            if (i >= a.n) continue;
+            const T q = a.charges[i];
+            if (q == T(0)) continue;
+            T r0[NDIM], r1[NDIM];
+            if (!path_cells<T, NDIM, WHITNEY>(a, i, r0, r1)) continue;
+            if constexpr (WHITNEY) whitney_path<T, NDIM>(q, r0, r1, a.g, sink);
+            else spline_path<T, NDIM, P>(q, r0, r1, a.g, sink);
+        }
+        __syncthreads();
+    }
+    if (have_box) flush_edge_box<T, NDIM>(tile, a.edges_out, sink, a.g);
 }
 
 // One thread per path, global atomics.

@@ -149,6 +149,23 @@ __device__ __forceinline__ int clamped_cell(T rel, int num, T* w) {
     return cell;
 }
 
+// The uniform spline stencil of degree P of rel on a periodic or bounded axis: returns the
+// pre-mapping first node and sets t, the offset of rel from the stencil's middle node
+// (the weights are uniform_weights<P>(t)).
+template <typename T, int P>
+__device__ __forceinline__ int spline_frame(T rel, int num, int code, T& t) {
+    if (code == PERIODIC) {
+        if (!(rel >= T(0) && rel < T(num))) rel = wrap_period(rel, num);
+    } else {
+        if (rel < T(0)) rel = T(0);
+        if (rel > T(num - 1)) rel = T(num - 1);
+    }
+    int middle = (P % 2 == 0) ? trunc_int<T>(rel + T(0.5)) : trunc_int<T>(rel);
+    middle = clampi(middle, 0, num);
+    t = rel - T(middle);
+    return middle - P / 2;
+}
+
 // The stencil of rel (the position in cells from the first node) along one axis: the
 // pre-mapping base node, and the weights w[0..P]. KIND LINEAR needs P == 1, QUADRATIC
 // P == 2; SPLINE takes P = 0..3 (clamped axes P >= 1).
@@ -186,16 +203,10 @@ __device__ __forceinline__ int axis_stencil(T rel, int num, int code, T* w) {
         if constexpr (P >= 1) {
             if (code == CLAMPED) return clamped_cell<T, P, false>(rel, num, w);
         }
-        if (code == PERIODIC) {
-            if (!(rel >= T(0) && rel < T(num))) rel = wrap_period(rel, num);
-        } else {
-            if (rel < T(0)) rel = T(0);
-            if (rel > T(num - 1)) rel = T(num - 1);
-        }
-        int middle = (P % 2 == 0) ? trunc_int<T>(rel + T(0.5)) : trunc_int<T>(rel);
-        middle = clampi(middle, 0, num);
-        uniform_weights<T, P>(rel - T(middle), w);
-        return middle - P / 2;
+        T t;
+        const int first = spline_frame<T, P>(rel, num, code, t);
+        uniform_weights<T, P>(t, w);
+        return first;
     }
 }
 

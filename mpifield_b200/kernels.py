@@ -157,6 +157,34 @@ def scatter(kind: int, degree: int, positions: torch.Tensor, values: torch.Tenso
     out.finish()
 
 
+def scatter_deterministic(kind: int, degree: int, positions: torch.Tensor, values: torch.Tensor,
+                          field: torch.Tensor, geometry, workspace: torch.Tensor | None = None) -> None:
+    """field(k, c) += sum_i W_k(x_i) values(c, i), the same bits for every run and marker
+    order (``mpf_scatter_deterministic``: fixed-point integer sums); float64 only."""
+    lower, cell, num, code, ndim = _lib.geometry_arrays(geometry)
+    device = _lib.require_cuda(positions, values, field)
+    if field.dtype != torch.float64:
+        raise TypeError("the deterministic scatter is float64 only")
+    shaped = _field_shape(field, _extent(num, code, degree), "field")
+    ncomp = shaped.shape[-1]
+    pos, ps = _marker_rows(positions, ndim, "positions", torch.float64)
+    vals, vs = _marker_rows(values, ncomp, "values", torch.float64)
+    if vals.shape[1] != pos.shape[1]:
+        raise ValueError(f"{pos.shape[1]} positions and {vals.shape[1]} values")
+    size = C.c_size_t(0)
+    _lib.check(_lib.library().mpf_scatter_deterministic_workspace_bytes(shaped.numel(), C.byref(size)),
+               "scatter_deterministic_workspace_bytes")
+    if workspace is None or workspace.numel() * workspace.element_size() < size.value:
+        workspace = torch.empty(size.value, dtype=torch.uint8, device=device)
+    out = _Output(shaped, torch.float64, accumulate=True)
+    status = _lib.library().mpf_scatter_deterministic(
+        kind, degree, ndim, pos.data_ptr(), ps, vals.data_ptr(), vs, pos.shape[1], out.work.data_ptr(), ncomp,
+        lower, cell, num, code, workspace.data_ptr(), workspace.numel() * workspace.element_size(),
+        _lib.stream_of(device))
+    _lib.check(status, "scatter_deterministic")
+    out.finish()
+
+
 def gather_grad(kind: int, degree: int, positions: torch.Tensor, field: torch.Tensor,
                 cotangent: torch.Tensor, geometry) -> torch.Tensor:
     """``(ndim, N)``: d/dx_d of sum_c cotangent(c, i) gather_c(x_i), the position gradient."""
@@ -211,7 +239,7 @@ class EdgeGatherKernel:
 
 
 def deposit_paths(kind: int, degree: int, start: torch.Tensor, end: torch.Tensor, charges: torch.Tensor,
-                  edges: torch.Tensor, geometry) -> None:
+                  edges: torch.Tensor, geometry, tuning: _lib.Tuning | None = None) -> None:
     """edges += the current of ``charges`` moving from ``start`` to ``end`` (ndim, N)."""
     lower, cell, num, code, ndim = _lib.geometry_arrays(geometry)
     device = _lib.require_cuda(start, end, charges, edges)
@@ -227,7 +255,8 @@ def deposit_paths(kind: int, degree: int, start: torch.Tensor, end: torch.Tensor
     out = _Output(edges, dtype, accumulate=True)
     status = _lib.library().mpf_deposit_paths(
         kind, degree, ndim, s.data_ptr(), ss, e.data_ptr(), es, q.data_ptr(), q.shape[0],
-        out.work.data_ptr(), lower, cell, num, code, _lib.dtype_code(dtype), None, _lib.stream_of(device))
+        out.work.data_ptr(), lower, cell, num, code, _lib.dtype_code(dtype),
+        C.byref(tuning) if tuning is not None else None, _lib.stream_of(device))
     _lib.check(status, "deposit_paths")
     out.finish()
 

@@ -80,6 +80,14 @@ def test_invalid_arguments_return_a_status_before_any_device_work():
     stored = (C.c_int32 * 1)(3)
     per = (C.c_int32 * 1)(1)
     assert lib.mpf_halo_fold(fake, 1, stored, 1, 2, per, 0, None) == _lib.ERR_SHAPE
+    # the deterministic scatter: a workspace too small, misaligned
+    size = C.c_size_t()
+    assert lib.mpf_scatter_deterministic_workspace_bytes(8 * 8 * 8, C.byref(size)) == 0
+    assert size.value >= 2 * 8 * 512
+    assert lib.mpf_scatter_deterministic(1, 2, 3, fake, 0, fake, 0, 10, fake, 1, lower, cell, num, code, fake,
+                                         16, None) == _lib.ERR_WORKSPACE
+    assert lib.mpf_scatter_deterministic(1, 2, 3, fake, 0, fake, 0, 10, fake, 1, lower, cell, num, code, fake + 8,
+                                         size.value, None) == _lib.ERR_ALIGNMENT
     # a workspace too small
     t = (C.c_int32 * 3)(4, 4, 4)
     assert lib.mpf_sort_by_tile(1, 2, 3, fake, 0, None, 0, 0, 1000, lower, cell, num, code, t, 0, fake, fake, fake,

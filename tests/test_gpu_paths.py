@@ -27,9 +27,15 @@ def cu(a, dtype=torch.float64):
     return torch.as_tensor(np.ascontiguousarray(a), dtype=dtype, device=DEV)
 
 
-def run_deposit(kind, degree, start, end, charges, shape, geom, dtype=torch.float64):
+# one thread per path with global atomics (the default), the tiled deposit (shared-memory
+# edge boxes, path 2) and the same with boxes too small for most chunks
+TUNINGS = {"direct": None, "tiled": _lib.tuning_struct(_lib.PATH_STAGED),
+           "small_box": _lib.tuning_struct(_lib.PATH_STAGED, smem_bytes=2048, block=2)}
+
+
+def run_deposit(kind, degree, start, end, charges, shape, geom, dtype=torch.float64, tuning="direct"):
     edges = torch.zeros(shape, dtype=dtype, device=DEV)
-    deposit_paths(kind, degree, cu(start, dtype), cu(end, dtype), cu(charges, dtype), edges, geom)
+    deposit_paths(kind, degree, cu(start, dtype), cu(end, dtype), cu(charges, dtype), edges, geom, TUNINGS[tuning])
     return edges.double().cpu().numpy()
 
 
@@ -74,12 +80,14 @@ def test_random_paths_match_the_oracle_and_conserve_charge(ndim, degree):
             geom, start, end, charges, ext = _case(rng, ndim, codes, degree, 4000, reach)
             charges[::17] = 0.0
             expected = O.deposit_spline(degree, start, end, charges, np.zeros((*ext, ndim)), geom)
-            got = run_deposit(_lib.SPLINE, degree, start, end, charges, (*ext, ndim), geom)
-            np.testing.assert_allclose(got, expected, rtol=0, atol=1e-12 * np.abs(expected).max())
+            for tuning in TUNINGS:
+                got = run_deposit(_lib.SPLINE, degree, start, end, charges, (*ext, ndim), geom, tuning=tuning)
+                np.testing.assert_allclose(got, expected, rtol=0, atol=1e-12 * np.abs(expected).max())
             if degree == 1 and 2 not in codes:
                 expected = O.deposit_whitney(start, end, charges, np.zeros((*ext, ndim)), geom)
-                got = run_deposit(_lib.LINEAR, 1, start, end, charges, (*ext, ndim), geom)
-                np.testing.assert_allclose(got, expected, rtol=0, atol=1e-12 * np.abs(expected).max())
+                for tuning in TUNINGS:
+                    got = run_deposit(_lib.LINEAR, 1, start, end, charges, (*ext, ndim), geom, tuning=tuning)
+                    np.testing.assert_allclose(got, expected, rtol=0, atol=1e-12 * np.abs(expected).max())
             if 2 not in codes:
                 kind = "linear" if degree == 1 else ("quadratic" if degree == 2 else "spline")
                 before = O.scatter(kind, degree, start, charges[None], np.zeros((*ext, 1)), geom)
@@ -143,7 +151,14 @@ def test_full_size_continuity_128_cubed(degree):
     edges = torch.zeros((128, 128, 128, 3), dtype=torch.float64, device=DEV)
     ew = mf.splines(degree).edges
     nodes = mf.splines(degree).nodes
+    # sorted by the start's cell tile: the tiled deposit keeps its chunks in shared memory
+    order = mf.sort_by_tile(start, mf.LINEAR, grid.geometry, (8, 8, 8), within=True).order
+    start, end, q = mf.permute(start, order), mf.permute(end, order), mf.permute(q, order)
     ew.deposit_paths_block(start, end, q, edges, grid)
+    tiled = torch.zeros_like(edges)
+    deposit_paths(_lib.LINEAR if degree == 1 else _lib.SPLINE, degree, start, end, q, tiled, grid.geometry,
+                  TUNINGS["tiled"])
+    assert float((edges - tiled).abs().max()) < 1e-12 * float(edges.abs().max())
     before = torch.zeros((128, 128, 128, 1), dtype=torch.float64, device=DEV)
     after = torch.zeros_like(before)
     nodes.scatter_block(start, q, before, grid)
