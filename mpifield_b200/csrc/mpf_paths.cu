@@ -6,8 +6,8 @@
 
 namespace mpf {
 
-// One thread per path with global atomics (the default: the L2's native FP64 adds
-// measured faster than shared-memory boxes, whose FP64 adds are compare-and-swap loops),
+// One thread per path with global atomics (the default: the L2's FP64 adds measured
+// faster than shared-memory boxes here, where many lanes add to the same nodes),
 // or the tiled kernel (path 2, staged): chunks of 256 x t.block paths (8 when t.block is
 // 0), a box of edges in t.smem_bytes (96 KB when 0) of shared memory.
 template <typename T, int NDIM, int P, bool WHITNEY>
