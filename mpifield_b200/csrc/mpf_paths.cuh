@@ -372,140 +372,97 @@ __device__ void spline_path(T q, const T* r0, const T* r1, const Grid<T>& g, con
                         along_frame<T, P>(mid, g.num[d], g.code[d], aidx[d], aex[d], at[d]);
                     }
                     constexpr int SX = P + 1;
+                    constexpr int CB = NDIM > 1 ? SX : 1;
+                    constexpr int CC = NDIM > 2 ? SX : 1;
 #pragma unroll
                     for (int axis = 0; axis < NDIM; ++axis) {
                         if (q * step[axis] == T(0)) continue;
-                        const int cnt0 = axis == 0 ? P : SX;
-                        const int cnt1 = NDIM > 1 ? (axis == 1 ? P : SX) : 1;
-                        const int cnt2 = NDIM > 2 ? (axis == 2 ? P : SX) : 1;
-                        T acc[P * (NDIM > 1 ? SX : 1) * (NDIM > 2 ? SX : 1)];
+                        // the axes across this one, in increasing order
+                        const int o1 = NDIM > 1 ? (axis == 0 ? 1 : 0) : 0;
+                        const int o2 = NDIM > 2 ? (axis == 2 ? 1 : 2) : 0;
+                        // one edge along the axis at a time: (P + 1)^(ndim - 1) sums
 #pragma unroll
-                        for (int k = 0; k < cnt0 * cnt1 * cnt2; ++k) acc[k] = T(0);
+                        for (int e = 0; e < P; ++e) {
+                            if (!aex[axis][e]) continue;
+                            T acc[CB * CC];
 #pragma unroll
-                        for (int gp = 0; gp < NPTS; ++gp) {
-                            const T off = Gauss<T, NPTS>::point(gp) - T(0.5);
-                            const T amount = q * Gauss<T, NPTS>::weight(gp) * step[axis];
-                            T wt[3][P + 1];
+                            for (int k = 0; k < CB * CC; ++k) acc[k] = T(0);
 #pragma unroll
-                            for (int d = 0; d < NDIM; ++d) {
-                                if (d == axis) uniform_weights<T, P - 1>(at[d] + off * step[d], wt[d]);
-                                else uniform_weights<T, P>(st[d] + off * step[d], wt[d]);
-                            }
+                            for (int gp = 0; gp < NPTS; ++gp) {
+                                const T off = Gauss<T, NPTS>::point(gp) - T(0.5);
+                                T wa[P > 0 ? P : 1], wb[SX], wc[SX];
+                                uniform_weights<T, P - 1>(at[axis] + off * step[axis], wa);
+                                if constexpr (NDIM > 1) uniform_weights<T, P>(st[o1] + off * step[o1], wb);
+                                if constexpr (NDIM > 2) uniform_weights<T, P>(st[o2] + off * step[o2], wc);
+                                const T along = q * Gauss<T, NPTS>::weight(gp) * step[axis] * wa[e];
 #pragma unroll
-                            for (int x = 0; x < cnt0; ++x)
+                                for (int b = 0; b < CB; ++b) {
+                                    const T wab = NDIM > 1 ? along * wb[b] : along;
 #pragma unroll
-                                for (int y = 0; y < cnt1; ++y) {
-                                    T wxy = amount * wt[0][x];
-                                    if constexpr (NDIM > 1) wxy = wxy * wt[1][y];
-#pragma unroll
-                                    for (int z = 0; z < cnt2; ++z) {
-                                        T& r = acc[(x * cnt1 + y) * cnt2 + z];
-                                        if constexpr (NDIM > 2) r = fma(wxy, wt[2][z], r);
-                                        else r = r + wxy;
+                                    for (int c = 0; c < CC; ++c) {
+                                        T& r = acc[b * CC + c];
+                                        if constexpr (NDIM > 2) r = fma(wab, wc[c], r);
+                                        else r = r + wab;
                                     }
                                 }
-                        }
-#pragma unroll
-                        for (int x = 0; x < cnt0; ++x) {
-                            if (axis == 0 && !aex[0][x]) continue;
-#pragma unroll
-                            for (int y = 0; y < cnt1; ++y) {
-                                if (NDIM > 1 && axis == 1 && !aex[1][y]) continue;
-#pragma unroll
-                                for (int z = 0; z < cnt2; ++z) {
-                                    if (NDIM > 2 && axis == 2 && !aex[2][z]) continue;
-                                    int n[3];
-                                    n[0] = axis == 0 ? aidx[0][x] : sidx[0][x];
-                                    n[1] = NDIM > 1 ? (axis == 1 ? aidx[1][y] : sidx[1][y]) : 0;
-                                    n[2] = NDIM > 2 ? (axis == 2 ? aidx[2][z] : sidx[2][z]) : 0;
-                                    sink.add(n, axis, acc[(x * cnt1 + y) * cnt2 + z]);
-                                }
                             }
+#pragma unroll
+                            for (int b = 0; b < CB; ++b)
+#pragma unroll
+                                for (int c = 0; c < CC; ++c) {
+                                    int n[3] = {0, 0, 0};
+                                    n[axis] = aidx[axis][e];
+                                    if constexpr (NDIM > 1) n[o1] = sidx[o1][b];
+                                    if constexpr (NDIM > 2) n[o2] = sidx[o2][c];
+                                    sink.add(n, axis, acc[b * CC + c]);
+                                }
                         }
                     }
                 } else {
-                    // The Gauss points of a piece lie in one knot interval on every axis, so
-                    // they share the edges of their stencils: their contributions are summed
-                    // in registers and added once per piece and axis (a point whose stencil
-                    // differs -- rounding at a cut -- closes the sum and opens a new one).
-                    constexpr int SX = P + 1;
-                    constexpr int CNT = P * (NDIM > 1 ? SX : 1) * (NDIM > 2 ? SX : 1);
-    #pragma unroll
-                    for (int axis = 0; axis < NDIM; ++axis) {
-                        T acc[CNT];
-                        int cur[3][P + 1];
-                        bool cur_ex[P > 0 ? P : 1];
-                        bool open = false;
-                        const int cnt0 = axis == 0 ? P : SX;
-                        const int cnt1 = NDIM > 1 ? (axis == 1 ? P : SX) : 1;
-                        const int cnt2 = NDIM > 2 ? (axis == 2 ? P : SX) : 1;
-                        auto flush = [&]() {
-    #pragma unroll
-                            for (int x = 0; x < cnt0; ++x) {
-                                if (axis == 0 && !cur_ex[x]) continue;
-    #pragma unroll
-                                for (int y = 0; y < cnt1; ++y) {
-                                    if (NDIM > 1 && axis == 1 && !cur_ex[y]) continue;
-    #pragma unroll
-                                    for (int z = 0; z < cnt2; ++z) {
-                                        if (NDIM > 2 && axis == 2 && !cur_ex[z]) continue;
-                                        int n[3] = {cur[0][x], NDIM > 1 ? cur[1][y] : 0, NDIM > 2 ? cur[2][z] : 0};
-                                        sink.add(n, axis, acc[(x * cnt1 + y) * cnt2 + z]);
-                                    }
-                                }
-                            }
-                        };
-    #pragma unroll
-                        for (int gp = 0; gp < NPTS; ++gp) {
-                            const T point = Gauss<T, NPTS>::point(gp);
-                            const T gw = Gauss<T, NPTS>::weight(gp);
+                    // clamped knots: every Gauss point computes its full stencil (Cox-de Boor
+                    // near the walls) and adds its own contributions
+#pragma unroll
+                    for (int gp = 0; gp < NPTS; ++gp) {
+                        const T point = Gauss<T, NPTS>::point(gp);
+                        const T gw = Gauss<T, NPTS>::weight(gp);
+                        T rel[NDIM];
+#pragma unroll
+                        for (int d = 0; d < NDIM; ++d) rel[d] = p0[d] + point * step[d];
+#pragma unroll 1
+                        for (int axis = 0; axis < NDIM; ++axis) {
                             const T amount = q * gw * step[axis];
                             if (amount == T(0)) continue;
                             int idx[3][P + 1];
                             T wt[3][P + 1];
                             bool ex[P > 0 ? P : 1];
-    #pragma unroll
+#pragma unroll
                             for (int d = 0; d < NDIM; ++d) {
-                                const T rel = p0[d] + point * step[d];
                                 if (d == axis) {
-                                    along_stencil<T, P>(rel, g.num[d], g.code[d], idx[d], wt[d], ex);
+                                    along_stencil<T, P>(rel[d], g.num[d], g.code[d], idx[d], wt[d], ex);
                                 } else {
-                                    const int base = axis_stencil<T, SPLINE, P>(rel, g.num[d], g.code[d], wt[d]);
-    #pragma unroll
-                                    for (int s = 0; s <= P; ++s) idx[d][s] = map_node(base + s, g.num[d], g.code[d]);
+                                    const int base = axis_stencil<T, SPLINE, P>(rel[d], g.num[d], g.code[d], wt[d]);
+#pragma unroll
+                                    for (int s2 = 0; s2 <= P; ++s2) idx[d][s2] = map_node(base + s2, g.num[d], g.code[d]);
                                 }
                             }
-                            bool same = open;
-    #pragma unroll
-                            for (int d = 0; d < NDIM; ++d)
-    #pragma unroll
-                                for (int s = 0; s <= P; ++s) same = same && idx[d][s] == cur[d][s];
-    #pragma unroll
-                            for (int s = 0; s < (P > 0 ? P : 1); ++s) same = same && ex[s] == cur_ex[s];
-                            if (!same) {
-                                if (open) flush();
-    #pragma unroll
-                                for (int d = 0; d < NDIM; ++d)
-    #pragma unroll
-                                    for (int s = 0; s <= P; ++s) cur[d][s] = idx[d][s];
-    #pragma unroll
-                                for (int s = 0; s < (P > 0 ? P : 1); ++s) cur_ex[s] = ex[s];
-                                open = true;
-                            }
-    #pragma unroll
-                            for (int x = 0; x < cnt0; ++x)
-    #pragma unroll
-                                for (int y = 0; y < cnt1; ++y)
-    #pragma unroll
+                            const int cnt0 = axis == 0 ? P : P + 1;
+                            const int cnt1 = NDIM > 1 ? (axis == 1 ? P : P + 1) : 1;
+                            const int cnt2 = NDIM > 2 ? (axis == 2 ? P : P + 1) : 1;
+                            for (int x = 0; x < cnt0; ++x) {
+                                if (axis == 0 && !ex[x]) continue;
+                                for (int y = 0; y < cnt1; ++y) {
+                                    if (NDIM > 1 && axis == 1 && !ex[y]) continue;
                                     for (int z = 0; z < cnt2; ++z) {
+                                        if (NDIM > 2 && axis == 2 && !ex[z]) continue;
                                         T w = amount * wt[0][x];
                                         if constexpr (NDIM > 1) w = w * wt[1][y];
                                         if constexpr (NDIM > 2) w = w * wt[2][z];
-                                        T& r = acc[(x * cnt1 + y) * cnt2 + z];
-                                        r = same ? r + w : w;
+                                        int n[3] = {idx[0][x], NDIM > 1 ? idx[1][y] : 0, NDIM > 2 ? idx[2][z] : 0};
+                                        sink.add(n, axis, w);
                                     }
+                                }
+                            }
                         }
-                        if (open) flush();
                     }
                 }
                 t0 = t1;
@@ -755,7 +712,7 @@ __global__ void __launch_bounds__(256) deposit_paths_tiled_kernel(const PathArgs
 
 // One thread per path, global atomics.
 template <typename T, int NDIM, int P, bool WHITNEY>
-__global__ void __launch_bounds__(256) deposit_paths_kernel(const PathArgs<T> a) {
+__global__ void __launch_bounds__(256, 1) deposit_paths_kernel(const PathArgs<T> a) {
     GlobalEdgeSink<T, NDIM> sink;
     sink.edges = a.edges_out;
 #pragma unroll
