@@ -69,7 +69,8 @@ def parse() -> argparse.Namespace:
     p.add_argument("--serve-requests", type=int, default=1000, help="requests of the serving stream (0: skip)")
     p.add_argument("--paths-only", type=int, default=0, metavar="N",
                    help="measure only the path deposits, at N paths on 128^3 (a profiling case)")
-    p.add_argument("--serve-rate", type=float, default=2000.0, help="Poisson arrival rate of the stream, per s")
+    p.add_argument("--serve-rate", type=float, default=20000.0,
+                   help="Poisson arrival rate of the stream, per s (the default outruns both arms: capacity)")
     return p.parse_args()
 
 
