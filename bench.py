@@ -244,20 +244,25 @@ class Step:
         self.E = torch.empty((3, n), dtype=dtype, device=device)
         self.E_out = torch.empty((3, n), dtype=dtype, device=device)
         self.kernels = (mf.KERNELS["gather_quadratic_3d"], mf.KERNELS["scatter_quadratic_3d"])
+        self.order = None
 
     def sort(self, pos, w):
+        """Sorts the markers by cell tile; the store keeps the order (its tile starts)."""
         t = self.mf.sort_by_tile(pos, self.mf.QUADRATIC, self.geom, TILE, within=True)
+        self.order = t
         return t, self.mf.permute(pos, t.order), self.mf.permute(w, t.order)
 
     def gather_scatter(self, pos, w, events=None):
-        gather, scatter = self.kernels
+        """Gather E and scatter the weights on the sorted store (the scatter takes the
+        store's tile starts: mpf_scatter_tiles)."""
+        gather, _ = self.kernels
         if events is not None:
             events[0].record()
         gather(pos, self.field, self.E, *self.geom)
         if events is not None:
             events[1].record()
         self.density.zero_()
-        scatter(pos, w, self.density, *self.geom)
+        self.mf.kernels.scatter(self.lib.QUADRATIC, 2, pos, w, self.density, self.geom, order=self.order)
         if events is not None:
             events[2].record()
 

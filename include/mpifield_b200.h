@@ -118,6 +118,24 @@ MPF_API int mpf_scatter(int kind, int degree, int ndim, const void* positions, i
                 const double* lower, const double* cell, const int32_t* num, const int32_t* code,
                 int dtype, const mpf_tuning* tuning, void* stream);
 
+/*
+ * mpf_scatter for markers sorted by cell tile: positions and values in the rank order of
+ * mpf_sort_by_tile (keys of the same kind, degree, geometry and `tile`, `within` either
+ * way), tile_start its num_tiles + 2 starts (8-byte aligned device memory). The result
+ * is mpf_scatter's on the same arguments up to the order of the floating-point adds,
+ * whatever the order of the markers: a marker outside its rank's tile adds to global
+ * memory directly. With one component, every axis periodic and a stencil of at most 27
+ * points, each tile's share of the markers is summed in a shared-memory box known from
+ * the tile (no per-chunk box search); other shapes, and tuning->variant != 0, run
+ * mpf_scatter's kernels. No counterpart in the reference, which scatters in marker
+ * order (src/mpifield/weighting.py:195-213).
+ */
+MPF_API int mpf_scatter_tiles(int kind, int degree, int ndim, const void* positions, int64_t pos_stride,
+                              const void* values, int64_t val_stride, int64_t n, void* field, int64_t ncomp,
+                              const double* lower, const double* cell, const int32_t* num,
+                              const int32_t* code, const int32_t* tile, const int64_t* tile_start,
+                              int dtype, const mpf_tuning* tuning, void* stream);
+
 /* Bytes of the workspace of mpf_scatter_deterministic for a field of `entries` values
  * (the product of its extent and ncomp). */
 MPF_API int mpf_scatter_deterministic_workspace_bytes(int64_t entries, size_t* bytes);

@@ -235,6 +235,48 @@ int mpf_scatter(int kind, int degree, int ndim, const void* positions, int64_t p
     return launch_scatter<float>(kind, degree, ndim, a, t, s);
 }
 
+int mpf_scatter_tiles(int kind, int degree, int ndim, const void* positions, int64_t pos_stride, const void* values,
+                      int64_t val_stride, int64_t n, void* field, int64_t ncomp, const double* lower,
+                      const double* cell, const int32_t* num, const int32_t* code, const int32_t* tile,
+                      const int64_t* tile_start, int dtype, const mpf_tuning* tuning, void* stream) {
+    if (!valid_kind(kind, degree) || (dtype != MPF_F64 && dtype != MPF_F32)) return MPF_ERR_ARGUMENT;
+    MPF_TRY(check_grid(kind, degree, ndim, lower, cell, num, code));
+    if (n < 0 || ncomp < 1 || ncomp > (1 << 20)) return MPF_ERR_ARGUMENT;
+    MPF_TRY(check_rows(positions, pos_stride, n, ndim, dtype));
+    MPF_TRY(check_rows(values, val_stride, n, (int)ncomp, dtype));
+    int64_t ntiles = 0;
+    MPF_TRY(mpf_num_tiles(kind, degree, ndim, num, code, tile, &ntiles));
+    if (!tile_start) return MPF_ERR_ARGUMENT;
+    if (reinterpret_cast<uintptr_t>(tile_start) % alignof(int64_t) != 0) return MPF_ERR_ALIGNMENT;
+    if (n == 0) return MPF_OK;
+    if (!field) return MPF_ERR_ARGUMENT;
+    if (!aligned(field, dtype)) return MPF_ERR_ALIGNMENT;
+    const Tuning t = tuning_of(tuning);
+    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    auto sorted = [&](auto& a) {
+        a.tile_start = tile_start;
+        a.ntiles = ntiles;
+        for (int d = 0; d < ndim; ++d) {
+            a.tile[d] = tile[d];
+            a.tiles[d] = (int)((axis_extent(num[d], code[d], degree) + tile[d] - 1) / tile[d]);
+        }
+    };
+    if (dtype == MPF_F64) {
+        NodeArgs<double> a = node_args<double>(ndim, degree, lower, cell, num, code);
+        a.pos = (const double*)positions; a.pos_stride = pos_stride;
+        a.values = (const double*)values; a.val_stride = val_stride;
+        a.field_out = (double*)field; a.n = n; a.ncomp = (int)ncomp;
+        sorted(a);
+        return launch_scatter<double>(kind, degree, ndim, a, t, s);
+    }
+    NodeArgs<float> a = node_args<float>(ndim, degree, lower, cell, num, code);
+    a.pos = (const float*)positions; a.pos_stride = pos_stride;
+    a.values = (const float*)values; a.val_stride = val_stride;
+    a.field_out = (float*)field; a.n = n; a.ncomp = (int)ncomp;
+    sorted(a);
+    return launch_scatter<float>(kind, degree, ndim, a, t, s);
+}
+
 int mpf_scatter_deterministic_workspace_bytes(int64_t entries, size_t* bytes) {
     if (entries < 0 || !bytes) return MPF_ERR_ARGUMENT;
     *bytes = det_workspace_bytes(entries);

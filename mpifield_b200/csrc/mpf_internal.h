@@ -35,6 +35,11 @@ template <typename T> struct NodeArgs {
     int force_global;    // 1: never stage (the direct path), for tests and unsorted input
     int bulk;            // 1: positions are 16-byte aligned rows, prefetched by bulk copies
     unsigned* error;     // device word of MPF_DEVICE_ERROR_* bits
+    // a scatter of markers sorted by cell tile (mpf_sort_by_tile); tile_start null otherwise
+    const int64_t* tile_start;  // first rank of every tile, then of the sentinel tile
+    int64_t ntiles;
+    int tile[3];         // anchor nodes per tile, per axis
+    int tiles[3];        // tiles per axis
 };
 
 // The tuning of one launch (the autotuned table supplies it; zero fields take defaults).

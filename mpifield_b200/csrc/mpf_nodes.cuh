@@ -844,6 +844,264 @@ __global__ void __launch_bounds__(kMaxBlock, MINB) scatter_segments_kernel(const
     if (have_box) flush_box<T, NDIM, 1>(tile, a.field_out, box, a.g, 1);
 }
 
+// ------------------------------------------------------- the tile scatter (sorted) --
+
+// The tile holding rank m, searched from tile `t` (tile_start[t] <= m): the tile whose
+// ranks reach past m, tile_start[t + 1] > m. A store sorted by tile mostly needs the
+// next tile or the one after, so a few steps forward come first, then a binary search.
+// Always a tile in [0, ntiles).
+__device__ __forceinline__ int64_t tile_of(const int64_t* ts, int64_t ntiles, int64_t t, int64_t m) {
+    t = min(max(t, (int64_t)0), ntiles - 1);
+#pragma unroll 1
+    for (int step = 0; step < 4; ++step, ++t)
+        if (t + 1 >= ntiles || __ldg(ts + t + 1) > m) return t;
+    int64_t lo = t, hi = ntiles - 1;  // the last tile in [t, ntiles) starting at or before m
+#pragma unroll 1
+    while (lo < hi) {
+        const int64_t mid = lo + (hi - lo + 1) / 2;
+        if (__ldg(ts + mid) <= m) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// The extents of the box of a tile (tile + P nodes per axis, the last made odd so that
+// nodes a whole number of rows apart fall in different shared-memory banks).
+template <int NDIM, int P>
+__device__ __forceinline__ void tile_box_extents(const int* tile, int* ex) {
+#pragma unroll
+    for (int d = 0; d < NDIM; ++d) ex[d] = tile[d] + P;
+    if ((ex[NDIM - 1] & 1) == 0) ++ex[NDIM - 1];
+}
+
+// field += the non-zero entries of a tile's box (global atomics), and the box zeroed.
+// The box is row-major with extents ex; its entry (0, 0, 0) is the pre-mapping node lo
+// of a grid whose axes are all periodic. Thread t takes entries t, t + B, t + 2B, ...
+// (B = blockDim.x), its box coordinates found once and then advanced by those of B with
+// one carry per axis: no division per entry.
+template <typename T, int NDIM>
+__device__ __forceinline__ void flush_clear_box(T* box, T* field, const int* lo, const int* ex, const Grid<T>& g) {
+    int total = 1;
+#pragma unroll
+    for (int d = 0; d < NDIM; ++d) total *= ex[d];
+    int c[3] = {0, 0, 0}, dc[3] = {0, 0, 0};
+    int q = threadIdx.x, b = blockDim.x;
+#pragma unroll
+    for (int d = NDIM - 1; d > 0; --d) {
+        c[d] = q % ex[d];
+        q /= ex[d];
+        dc[d] = b % ex[d];
+        b /= ex[d];
+    }
+    c[0] = q;
+    dc[0] = b;
+#pragma unroll 1
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+        const T v = box[e];
+        if (v != T(0)) {
+            box[e] = T(0);
+            int64_t at = 0;
+#pragma unroll
+            for (int d = 0; d < NDIM; ++d) at = at * g.ext[d] + wrap_index(lo[d] + c[d], g.num[d]);
+            atomicAdd(field + at, v);
+        }
+        int carry = 0;
+#pragma unroll
+        for (int d = NDIM - 1; d >= 0; --d) {
+            c[d] += dc[d] + carry;
+            carry = 0;
+            if (d > 0 && c[d] >= ex[d]) {
+                c[d] -= ex[d];
+                carry = 1;
+            }
+        }
+    }
+}
+
+// The tile scatter: the segment scatter (above) for markers sorted by cell tile
+// (mpf_sort_by_tile), one component, every axis periodic. tile_start names the ranks of
+// every tile, so the CTA's share of the ranks (an equal share of the live markers, the
+// tiles before the sentinel) splits at tile boundaries into pieces whose box is known
+// in advance: the tile's anchors widened by the stencil, tile + P nodes per axis (the
+// last axis made odd for the shared-memory banks). No box reduction, no frame choice,
+// one flush per piece, fused with the zeroing. A piece is cut into nearly equal
+// sub-chunks of at most 256 x K markers, thread t owning the contiguous markers
+// t kq .. t kq + kq - 1 (kq = ceil(count / 256)) in the padded rows of the segment
+// scatter. Runs of one anchor are summed in registers and added to the box as there.
+// A marker whose anchor is not in the piece's tile (tile_start not made from these
+// positions) adds to global memory directly: the result never depends on the order.
+template <typename T, int NDIM, int KIND, int P, int K, int MINB>
+__global__ void __launch_bounds__(kMaxBlock, MINB) scatter_tiles_kernel(const NodeArgs<T> a) {
+    constexpr int S = P + 1;
+    constexpr int SY = NDIM > 1 ? S : 1;
+    constexpr int SZ = NDIM > 2 ? S : 1;
+    constexpr int SP = S * SY * SZ;
+    constexpr int PITCH = K + 1;
+    constexpr int ROWS = NDIM + 1;
+    constexpr int CH = kMaxBlock * K;
+    constexpr int ROW = kMaxBlock * PITCH;
+    constexpr int H = P / 2;  // a stencil's anchor is its first node + H
+    constexpr unsigned FULL = 0xffffffffu;
+    T* buf = reinterpret_cast<T*>(mpf_dynamic_smem);  // [ROWS][ROW]
+    T* box = buf + ROWS * ROW;
+    const int t = threadIdx.x;
+    const int lane = t & 31;
+    {
+        int ex[3] = {1, 1, 1};
+        tile_box_extents<NDIM, P>(a.tile, ex);
+        for (int q = t; q < ex[0] * ex[1] * ex[2]; q += kMaxBlock) box[q] = T(0);
+    }
+    const int64_t live = min(max(__ldg(a.tile_start + a.ntiles), (int64_t)0), a.n);
+    const int64_t per = (live + gridDim.x - 1) / gridDim.x;
+    int64_t m = min((int64_t)blockIdx.x * per, live);
+    const int64_t m_end = min(m + per, live);
+    int64_t cur = -1;        // the tile of the box
+    int blo[3] = {0, 0, 0};  // its first anchor, per axis
+    // adds the box to the field, empties it, and makes it tile tt's
+    auto retire = [&](int64_t tt) {
+        if (cur >= 0) {
+            int ex[3] = {1, 1, 1}, lo[3] = {0, 0, 0};
+            tile_box_extents<NDIM, P>(a.tile, ex);
+#pragma unroll
+            for (int d = 0; d < NDIM; ++d) lo[d] = blo[d] - H;
+            flush_clear_box<T, NDIM>(box, a.field_out, lo, ex, a.g);
+        }
+        cur = tt;
+        int64_t rest = tt;
+#pragma unroll
+        for (int d = NDIM - 1; d >= 0; --d) {
+            const int64_t c = rest % a.tiles[d];
+            rest /= a.tiles[d];
+            blo[d] = (int)c * a.tile[d];
+        }
+    };
+    while (m < m_end) {
+        const int64_t tt = tile_of(a.tile_start, a.ntiles, cur, m);
+        const int64_t e = min(m_end, max(m + 1, __ldg(a.tile_start + tt + 1)));
+        if (tt != cur) {
+            const bool had = cur >= 0;
+            retire(tt);
+            if (had) __syncthreads();
+        }
+        const int64_t len = e - m;
+        const int nsub = (int)((len + CH - 1) / CH);
+        const int64_t part = len / nsub, extra = len % nsub;
+#pragma unroll 1
+        for (int sub = 0; sub < nsub; ++sub) {
+            const int64_t first = m + sub * part + min((int64_t)sub, extra);
+            const int count = (int)(part + (sub < extra ? 1 : 0));
+            for (int j = t; j < count; j += kMaxBlock) {
+                const int q = (j / K) * PITCH + j % K;
+#pragma unroll
+                for (int d = 0; d < NDIM; ++d)
+                    cp_async<sizeof(T)>(buf + d * ROW + q, a.pos + d * a.pos_stride + first + j);
+                cp_async<sizeof(T)>(buf + NDIM * ROW + q, a.values + first + j);
+            }
+            cp_async_commit();
+            cp_async_wait_all();
+            __syncthreads();
+            const int kq = (count + kMaxBlock - 1) / kMaxBlock;
+            const int j0 = t * kq;
+            const int nmine = min(kq, max(0, count - j0));
+            // box strides: node (x, y, z) of anchor key is box[key + x sa + y sb + z se]
+            int ex[3] = {1, 1, 1};
+            tile_box_extents<NDIM, P>(a.tile, ex);
+            const int se = NDIM > 2 ? 1 : 0;
+            const int sb = NDIM > 2 ? ex[2] : (NDIM > 1 ? 1 : 0);
+            const int sa = NDIM > 2 ? ex[1] * ex[2] : (NDIM > 1 ? ex[1] : 1);
+            const int st[3] = {sa, NDIM > 1 ? sb : 0, NDIM > 2 ? se : 0};
+            T acc[SP];
+#pragma unroll
+            for (int q = 0; q < SP; ++q) acc[q] = T(0);
+            int key = -1;  // the anchor of the open run, -1: none
+            // adds the open run to the box and empties it
+            auto flush = [&](int at) {
+#pragma unroll
+                for (int x = 0; x < S; ++x)
+#pragma unroll
+                    for (int y = 0; y < SY; ++y)
+#pragma unroll
+                        for (int z = 0; z < SZ; ++z) {
+                            atomicAdd(box + at + x * sa + y * sb + z * se, acc[(x * SY + y) * SZ + z]);
+                            acc[(x * SY + y) * SZ + z] = T(0);
+                        }
+            };
+#pragma unroll 1
+            for (int s = 0; s < nmine; ++s) {
+                const int j = j0 + s;
+                const int q = (j / K) * PITCH + j % K;
+                const T v = buf[NDIM * ROW + q];
+                if (v == T(0)) continue;
+                T w[3][S];
+                int base[3] = {0, 0, 0};
+                int k = 0;
+                bool inside = true;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    if (d < NDIM) {
+                        const T rel = rel_from(buf[d * ROW + q], a.g, d);
+                        base[d] = axis_stencil<T, KIND, P>(rel, a.g.num[d], PERIODIC, w[d]);
+                        const int off = wrap_index(base[d] + H - blo[d], a.g.num[d]);
+                        inside = inside && (unsigned)off < (unsigned)a.tile[d];
+                        k += off * st[d];
+                    } else {
+#pragma unroll
+                        for (int z = 0; z < S; ++z) w[d][z] = T(z == 0);
+                    }
+                }
+                if (!inside) {  // not this tile's marker: straight to global memory
+                    int64_t goff[3][S];
+                    global_offsets<NDIM, S>(base, a.g.num, a.g.code, a.g.ext, goff);
+                    const T vv[1] = {v};
+                    stencil_add<T, NDIM, S, 1, int64_t>(a.field_out, goff, w, 1, 0, vv);
+                    continue;
+                }
+                if (k != key && key >= 0) flush(key);
+                T wz[SZ];
+#pragma unroll
+                for (int z = 0; z < SZ; ++z) wz[z] = (NDIM > 2 ? w[2][z] : T(1)) * v;
+#pragma unroll
+                for (int x = 0; x < S; ++x)
+#pragma unroll
+                    for (int y = 0; y < SY; ++y) {
+                        const T wxy = NDIM > 2 ? w[0][x] * w[1][y] : (NDIM > 1 ? w[0][x] * (w[1][y] * v) : w[0][x] * v);
+#pragma unroll
+                        for (int z = 0; z < SZ; ++z) {
+                            T& r = acc[(x * SY + y) * SZ + z];
+                            r = NDIM > 2 ? fma(wxy, wz[z], r) : r + wxy;
+                        }
+                    }
+                key = k;
+            }
+            // the closing runs, as in the segment scatter
+            const int tag = key >= 0 ? key : -2 - lane;
+            const unsigned peers = __match_any_sync(FULL, tag);
+            const int head = __ffs(peers) - 1;
+            const int size = __popc(peers);
+            const int biggest = __reduce_max_sync(FULL, size);
+            const bool contiguous = peers == ((size == 32 ? FULL : ((1u << size) - 1u)) << head);
+            if (biggest >= 4 && __all_sync(FULL, contiguous)) {
+                const int last = head + size - 1;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+#pragma unroll
+                    for (int q = 0; q < SP; ++q) {
+                        const T other = __shfl_down_sync(FULL, acc[q], o);
+                        if (lane + o <= last) acc[q] += other;
+                    }
+                }
+                if (key >= 0 && lane == head) flush(key);
+            } else if (key >= 0) {
+                flush(key);
+            }
+            // the buffer is free, and the box complete, once every thread is past this point
+            __syncthreads();
+        }
+        m = e;
+    }
+    retire(-1);
+}
+
 // The scatter. The markers of a chunk go to warps in contiguous runs of 32 (lane l of
 // warp w, step s: marker (w * MPT + s) * 32 + l of the chunk), so that in a marker store
 // sorted by cell the lanes of a warp hold markers of a few cells. For a box chunk, every

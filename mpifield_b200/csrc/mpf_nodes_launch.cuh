@@ -116,13 +116,45 @@ static int run_scatter_segments(NodeArgs<T> a, const Tuning& t, cudaStream_t str
     return launch_status();
 }
 
-// Scatter variants: 0 (default) the segment scatter for one component and stencils of at
-// most 27 points, else the warp-transposed run reduction; 1 the segment scatter where it
-// applies; 2 the warp-transposed run reduction.
+// The tile scatter (markers sorted by cell tile, one component, periodic axes): 256
+// threads, MINB CTAs per SM, each CTA an equal share of the live markers. Returns
+// MPF_ERR_ARGUMENT, launching nothing, when the tile's box does not fit beside the rows.
+template <typename T, int NDIM, int KIND, int P, int K, int MINB>
+static int run_scatter_tiles(NodeArgs<T> a, cudaStream_t stream) {
+    const int buf_bytes = (NDIM + 1) * kMaxBlock * (K + 1) * (int)sizeof(T);
+    int64_t total = 1;
+    for (int d = 0; d < NDIM; ++d) {
+        int64_t e = (int64_t)a.tile[d] + P;
+        if (d == NDIM - 1 && (e & 1) == 0) ++e;
+        total *= e;
+    }
+    const int64_t box_bytes = total * (int64_t)sizeof(T);
+    if (box_bytes > (228 * 1024) / MINB - 2048 - buf_bytes) return MPF_ERR_ARGUMENT;
+    const int smem = buf_bytes + (int)box_bytes;
+    a.error = device_error_word();
+    if (!a.error) return MPF_ERR_CUDA;
+    auto kernel = scatter_tiles_kernel<T, NDIM, KIND, P, K, MINB>;
+    static int cache[64] = {0};
+    if (allow_smem(kernel, smem, cache) != MPF_OK) return MPF_ERR_CUDA;
+    const int64_t units = (a.n + kMaxBlock - 1) / kMaxBlock;
+    kernel<<<grid_for(units, smem, kMaxBlock, MINB), kMaxBlock, smem, stream>>>(a);
+    count_launches(1);
+    return launch_status();
+}
+
+// Scatter variants: 0 (default) the tile scatter for markers sorted by cell tile (one
+// component, periodic axes, stencils of at most 27 points, the tile's box within shared
+// memory), else the segment scatter for one component and stencils of at most 27
+// points, else the warp-transposed run reduction; 1 the segment scatter where it
+// applies (tile order ignored); 2 the warp-transposed run reduction.
 template <typename T, int NDIM, int KIND, int P, int NC>
 static int run_scatter(NodeArgs<T> a, const Tuning& t, cudaStream_t stream) {
     constexpr int SP = StencilPoints<P + 1, NDIM>::value;
     if constexpr (NC == 1 && SP <= 27) {
+        if (a.tile_start && t.variant == 0 && t.path != 1 && all_periodic<T, NDIM>(a)) {
+            const int st = run_scatter_tiles<T, NDIM, KIND, P, kSegment, 2>(a, stream);
+            if (st != MPF_ERR_ARGUMENT) return st;
+        }
         if (t.variant == 3) return run_scatter_segments<T, NDIM, KIND, P, 4, 3>(a, t, stream);
         if (t.variant != 2) return run_scatter_segments<T, NDIM, KIND, P, kSegment, 2>(a, t, stream);
     }

@@ -136,8 +136,13 @@ def gather(kind: int, degree: int, positions: torch.Tensor, field: torch.Tensor,
 
 
 def scatter(kind: int, degree: int, positions: torch.Tensor, values: torch.Tensor, field: torch.Tensor,
-            geometry, tuning: _lib.Tuning | None = None) -> None:
-    """field(k, c) += sum_i W_k(x_i) values(c, i); dead markers (all values zero) skipped."""
+            geometry, tuning: _lib.Tuning | None = None, order=None) -> None:
+    """field(k, c) += sum_i W_k(x_i) values(c, i); dead markers (all values zero) skipped.
+
+    ``order``: the `sorting.TileOrder` whose rank order the markers are in (positions and
+    values permuted by ``order.order``), for ``mpf_scatter_tiles``; the result is the same
+    up to the order of the floating-point adds, whatever the markers' order.
+    """
     lower, cell, num, code, ndim = _lib.geometry_arrays(geometry)
     device = _lib.require_cuda(positions, values, field)
     dtype = field.dtype
@@ -149,10 +154,22 @@ def scatter(kind: int, degree: int, positions: torch.Tensor, values: torch.Tenso
     if vals.shape[1] != pos.shape[1]:
         raise ValueError(f"{pos.shape[1]} positions and {vals.shape[1]} values")
     out = _Output(shaped, dtype, accumulate=True)
-    status = _lib.library().mpf_scatter(
-        kind, degree, ndim, pos.data_ptr(), ps, vals.data_ptr(), vs, pos.shape[1], out.work.data_ptr(),
-        ncomp, lower, cell, num, code, dcode, C.byref(tuning) if tuning is not None else None,
-        _lib.stream_of(device))
+    tune = C.byref(tuning) if tuning is not None else None
+    if order is None:
+        status = _lib.library().mpf_scatter(
+            kind, degree, ndim, pos.data_ptr(), ps, vals.data_ptr(), vs, pos.shape[1], out.work.data_ptr(),
+            ncomp, lower, cell, num, code, dcode, tune, _lib.stream_of(device))
+    else:
+        starts = order.tile_start
+        if starts.device != device or starts.dtype != torch.int64 or not starts.is_contiguous():
+            raise ValueError("order.tile_start must be a contiguous int64 tensor on the markers' device")
+        if len(order.tile) != ndim or starts.numel() != order.num_tiles + 2:
+            raise ValueError(f"a tile order of {len(order.tile)} axes and {starts.numel()} starts "
+                             f"for a {ndim}D grid")
+        tile = (C.c_int32 * ndim)(*(int(v) for v in order.tile))
+        status = _lib.library().mpf_scatter_tiles(
+            kind, degree, ndim, pos.data_ptr(), ps, vals.data_ptr(), vs, pos.shape[1], out.work.data_ptr(),
+            ncomp, lower, cell, num, code, tile, starts.data_ptr(), dcode, tune, _lib.stream_of(device))
     _lib.check(status, "scatter")
     out.finish()
 

@@ -30,6 +30,7 @@ class TileOrder:
     order: torch.Tensor       # (N,) int32: the marker of every rank
     tile_start: torch.Tensor  # (num_tiles + 2,) int64: first rank of every key, then N
     num_tiles: int
+    tile: tuple = ()          # anchor nodes per tile, per axis
 
 
 def _kind_of(weighting) -> tuple[int, int]:
@@ -92,7 +93,7 @@ def sort_by_tile(positions: torch.Tensor, weighting, geometry, tile, values: tor
         keys.data_ptr(), order.data_ptr(), tile_start.data_ptr(), workspace.data_ptr(), workspace.numel(),
         _lib.dtype_code(dtype), _lib.stream_of(device))
     _lib.check(status, "sort_by_tile")
-    return TileOrder(keys, order, tile_start, ntiles)
+    return TileOrder(keys, order, tile_start, ntiles, tuple(int(v) for v in tile))
 
 
 def permute(array: torch.Tensor, order: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:
