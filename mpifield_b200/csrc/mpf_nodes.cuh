@@ -927,10 +927,79 @@ __device__ __forceinline__ void flush_clear_box(T* box, T* field, const int* lo,
 // one flush per piece, fused with the zeroing. A piece is cut into nearly equal
 // sub-chunks of at most 256 x K markers, thread t owning the contiguous markers
 // t kq .. t kq + kq - 1 (kq = ceil(count / 256)) in the padded rows of the segment
-// scatter. Runs of one anchor are summed in registers and added to the box as there.
-// A marker whose anchor is not in the piece's tile (tile_start not made from these
-// positions) adds to global memory directly: the result never depends on the order.
-template <typename T, int NDIM, int KIND, int P, int K, int MINB>
+// scatter. Runs of one anchor are summed in registers and added to the box as there,
+// except that a run followed by the next cell along the last axis (anchor + 1, the
+// usual step in a store sorted by cell) adds only the plane of its window that the
+// next run does not touch and slides the rest: S^(NDIM-1) shared-memory atomics
+// instead of S^NDIM, the atomics being what the kernel's time goes to. Thread 0 plans
+// the sub-chunks; the plan and the loop state live in shared memory, not in the
+// registers of the marker loop. A marker whose anchor is not in the piece's tile
+// (tile_start not made from these positions) adds to global memory directly: the
+// result never depends on the order.
+struct TileLoop {
+    int64_t m, m_end;  // the next rank of the CTA's share, and its end
+    int64_t cur;       // the tile of the box (-1: none)
+    int64_t e;         // the end of the current piece
+    int64_t part, extra;
+    int sub, nsub;     // sub-chunks of the current piece: done, in all
+};
+struct TileStep {
+    int64_t first;  // the sub-chunk's first rank
+    int count;      // its markers (0: the CTA is done)
+    int retire;     // 1: add the box of the previous tile (first node old_lo) to the field first
+    int blo[3];     // the sub-chunk's tile: its first anchor per axis
+    int old_lo[3];
+};
+
+// Thread 0's plan of the next sub-chunk (tile pieces cut at tile_start, each into nearly
+// equal sub-chunks of at most ch markers).
+template <int NDIM, int H>
+__device__ __forceinline__ void plan_tile_step(TileLoop& L, TileStep& st, const int64_t* ts, int64_t ntiles,
+                                               const int* tiles, const int* tl, int ch) {
+    st.retire = 0;
+    if (L.sub >= L.nsub) {
+        L.m = L.e;
+        if (L.m >= L.m_end) {
+            st.count = 0;
+            st.retire = L.cur >= 0 ? 1 : 0;
+#pragma unroll
+            for (int d = 0; d < NDIM; ++d) st.old_lo[d] = st.blo[d] - H;
+            L.cur = -1;
+            return;
+        }
+        const int64_t tt = tile_of(ts, ntiles, L.cur, L.m);
+        L.e = min(L.m_end, max(L.m + 1, __ldg(ts + tt + 1)));
+        if (tt != L.cur) {
+            st.retire = L.cur >= 0 ? 1 : 0;
+            int rest = (int)tt;  // tiles number fewer than 2^31
+#pragma unroll
+            for (int d = NDIM - 1; d >= 0; --d) {
+                st.old_lo[d] = st.blo[d] - H;
+                const int c = rest % tiles[d];
+                rest /= tiles[d];
+                st.blo[d] = c * tl[d];
+            }
+            L.cur = tt;
+        }
+        const int64_t len = L.e - L.m;
+        if (len < ((int64_t)1 << 31)) {  // 32-bit divisions for the usual piece
+            const int n32 = (int)len;
+            L.nsub = (n32 + ch - 1) / ch;
+            L.part = n32 / L.nsub;
+            L.extra = n32 - (int)L.part * L.nsub;
+        } else {
+            L.nsub = (int)((len + ch - 1) / ch);
+            L.part = len / L.nsub;
+            L.extra = len % L.nsub;
+        }
+        L.sub = 0;
+    }
+    st.first = L.m + L.sub * L.part + min((int64_t)L.sub, L.extra);
+    st.count = (int)(L.part + (L.sub < L.extra ? 1 : 0));
+    ++L.sub;
+}
+
+template <typename T, int NDIM, int KIND, int P, int K, int MINB, int TX = 0, int TY = 0, int TZ = 0>
 __global__ void __launch_bounds__(kMaxBlock, MINB) scatter_tiles_kernel(const NodeArgs<T> a) {
     constexpr int S = P + 1;
     constexpr int SY = NDIM > 1 ? S : 1;
@@ -942,164 +1011,177 @@ __global__ void __launch_bounds__(kMaxBlock, MINB) scatter_tiles_kernel(const No
     constexpr int ROW = kMaxBlock * PITCH;
     constexpr int H = P / 2;  // a stencil's anchor is its first node + H
     constexpr unsigned FULL = 0xffffffffu;
+    __shared__ TileLoop s_loop;
+    __shared__ TileStep s_step;
     T* buf = reinterpret_cast<T*>(mpf_dynamic_smem);  // [ROWS][ROW]
     T* box = buf + ROWS * ROW;
     const int t = threadIdx.x;
     const int lane = t & 31;
-    {
-        int ex[3] = {1, 1, 1};
-        tile_box_extents<NDIM, P>(a.tile, ex);
-        for (int q = t; q < ex[0] * ex[1] * ex[2]; q += kMaxBlock) box[q] = T(0);
-    }
-    const int64_t live = min(max(__ldg(a.tile_start + a.ntiles), (int64_t)0), a.n);
-    const int64_t per = (live + gridDim.x - 1) / gridDim.x;
-    int64_t m = min((int64_t)blockIdx.x * per, live);
-    const int64_t m_end = min(m + per, live);
-    int64_t cur = -1;        // the tile of the box
-    int blo[3] = {0, 0, 0};  // its first anchor, per axis
-    // adds the box to the field, empties it, and makes it tile tt's
-    auto retire = [&](int64_t tt) {
-        if (cur >= 0) {
-            int ex[3] = {1, 1, 1}, lo[3] = {0, 0, 0};
-            tile_box_extents<NDIM, P>(a.tile, ex);
+    // the tile shape: compile-time constants where the launch fixes them (TX, TY, TZ > 0),
+    // so that the box strides and every stencil offset in the box are immediates
+    const int tl[3] = {TX > 0 ? TX : a.tile[0], TY > 0 ? TY : a.tile[1], TZ > 0 ? TZ : a.tile[2]};
+    int ex[3] = {1, 1, 1};
+    tile_box_extents<NDIM, P>(tl, ex);
+    for (int q = t; q < ex[0] * ex[1] * ex[2]; q += kMaxBlock) box[q] = T(0);
+    if (t == 0) {
+        const int64_t live = min(max(__ldg(a.tile_start + a.ntiles), (int64_t)0), a.n);
+        const int64_t per = (live + gridDim.x - 1) / gridDim.x;
+        s_loop.m = min((int64_t)blockIdx.x * per, live);
+        s_loop.m_end = min(s_loop.m + per, live);
+        s_loop.e = s_loop.m;
+        s_loop.cur = -1;
+        s_loop.sub = s_loop.nsub = 0;
+        s_loop.part = s_loop.extra = 0;
 #pragma unroll
-            for (int d = 0; d < NDIM; ++d) lo[d] = blo[d] - H;
+        for (int d = 0; d < 3; ++d) s_step.blo[d] = s_step.old_lo[d] = 0;
+    }
+    // box strides: node (x, y, z) of anchor key is box[key + x sa + y sb + z se]
+    const int se = NDIM > 2 ? 1 : 0;
+    const int sb = NDIM > 2 ? ex[2] : (NDIM > 1 ? 1 : 0);
+    const int sa = NDIM > 2 ? ex[1] * ex[2] : (NDIM > 1 ? ex[1] : 1);
+    const int st[3] = {sa, NDIM > 1 ? sb : 0, NDIM > 2 ? se : 0};
+#pragma unroll 1
+    for (;;) {
+        if (t == 0) plan_tile_step<NDIM, H>(s_loop, s_step, a.tile_start, a.ntiles, a.tiles, tl, CH);
+        // the plan is visible, the previous sub-chunk's adds are complete and its rows free
+        __syncthreads();
+        const int64_t first = s_step.first;
+        const int count = s_step.count;
+        if (s_step.retire) {
+            const int lo[3] = {s_step.old_lo[0], s_step.old_lo[1], s_step.old_lo[2]};
             flush_clear_box<T, NDIM>(box, a.field_out, lo, ex, a.g);
-        }
-        cur = tt;
-        int64_t rest = tt;
-#pragma unroll
-        for (int d = NDIM - 1; d >= 0; --d) {
-            const int64_t c = rest % a.tiles[d];
-            rest /= a.tiles[d];
-            blo[d] = (int)c * a.tile[d];
-        }
-    };
-    while (m < m_end) {
-        const int64_t tt = tile_of(a.tile_start, a.ntiles, cur, m);
-        const int64_t e = min(m_end, max(m + 1, __ldg(a.tile_start + tt + 1)));
-        if (tt != cur) {
-            const bool had = cur >= 0;
-            retire(tt);
-            if (had) __syncthreads();
-        }
-        const int64_t len = e - m;
-        const int nsub = (int)((len + CH - 1) / CH);
-        const int64_t part = len / nsub, extra = len % nsub;
-#pragma unroll 1
-        for (int sub = 0; sub < nsub; ++sub) {
-            const int64_t first = m + sub * part + min((int64_t)sub, extra);
-            const int count = (int)(part + (sub < extra ? 1 : 0));
-            for (int j = t; j < count; j += kMaxBlock) {
-                const int q = (j / K) * PITCH + j % K;
-#pragma unroll
-                for (int d = 0; d < NDIM; ++d)
-                    cp_async<sizeof(T)>(buf + d * ROW + q, a.pos + d * a.pos_stride + first + j);
-                cp_async<sizeof(T)>(buf + NDIM * ROW + q, a.values + first + j);
-            }
-            cp_async_commit();
-            cp_async_wait_all();
-            __syncthreads();
-            const int kq = (count + kMaxBlock - 1) / kMaxBlock;
-            const int j0 = t * kq;
-            const int nmine = min(kq, max(0, count - j0));
-            // box strides: node (x, y, z) of anchor key is box[key + x sa + y sb + z se]
-            int ex[3] = {1, 1, 1};
-            tile_box_extents<NDIM, P>(a.tile, ex);
-            const int se = NDIM > 2 ? 1 : 0;
-            const int sb = NDIM > 2 ? ex[2] : (NDIM > 1 ? 1 : 0);
-            const int sa = NDIM > 2 ? ex[1] * ex[2] : (NDIM > 1 ? ex[1] : 1);
-            const int st[3] = {sa, NDIM > 1 ? sb : 0, NDIM > 2 ? se : 0};
-            T acc[SP];
-#pragma unroll
-            for (int q = 0; q < SP; ++q) acc[q] = T(0);
-            int key = -1;  // the anchor of the open run, -1: none
-            // adds the open run to the box and empties it
-            auto flush = [&](int at) {
-#pragma unroll
-                for (int x = 0; x < S; ++x)
-#pragma unroll
-                    for (int y = 0; y < SY; ++y)
-#pragma unroll
-                        for (int z = 0; z < SZ; ++z) {
-                            atomicAdd(box + at + x * sa + y * sb + z * se, acc[(x * SY + y) * SZ + z]);
-                            acc[(x * SY + y) * SZ + z] = T(0);
-                        }
-            };
-#pragma unroll 1
-            for (int s = 0; s < nmine; ++s) {
-                const int j = j0 + s;
-                const int q = (j / K) * PITCH + j % K;
-                const T v = buf[NDIM * ROW + q];
-                if (v == T(0)) continue;
-                T w[3][S];
-                int base[3] = {0, 0, 0};
-                int k = 0;
-                bool inside = true;
-#pragma unroll
-                for (int d = 0; d < 3; ++d) {
-                    if (d < NDIM) {
-                        const T rel = rel_from(buf[d * ROW + q], a.g, d);
-                        base[d] = axis_stencil<T, KIND, P>(rel, a.g.num[d], PERIODIC, w[d]);
-                        const int off = wrap_index(base[d] + H - blo[d], a.g.num[d]);
-                        inside = inside && (unsigned)off < (unsigned)a.tile[d];
-                        k += off * st[d];
-                    } else {
-#pragma unroll
-                        for (int z = 0; z < S; ++z) w[d][z] = T(z == 0);
-                    }
-                }
-                if (!inside) {  // not this tile's marker: straight to global memory
-                    int64_t goff[3][S];
-                    global_offsets<NDIM, S>(base, a.g.num, a.g.code, a.g.ext, goff);
-                    const T vv[1] = {v};
-                    stencil_add<T, NDIM, S, 1, int64_t>(a.field_out, goff, w, 1, 0, vv);
-                    continue;
-                }
-                if (k != key && key >= 0) flush(key);
-                T wz[SZ];
-#pragma unroll
-                for (int z = 0; z < SZ; ++z) wz[z] = (NDIM > 2 ? w[2][z] : T(1)) * v;
-#pragma unroll
-                for (int x = 0; x < S; ++x)
-#pragma unroll
-                    for (int y = 0; y < SY; ++y) {
-                        const T wxy = NDIM > 2 ? w[0][x] * w[1][y] : (NDIM > 1 ? w[0][x] * (w[1][y] * v) : w[0][x] * v);
-#pragma unroll
-                        for (int z = 0; z < SZ; ++z) {
-                            T& r = acc[(x * SY + y) * SZ + z];
-                            r = NDIM > 2 ? fma(wxy, wz[z], r) : r + wxy;
-                        }
-                    }
-                key = k;
-            }
-            // the closing runs, as in the segment scatter
-            const int tag = key >= 0 ? key : -2 - lane;
-            const unsigned peers = __match_any_sync(FULL, tag);
-            const int head = __ffs(peers) - 1;
-            const int size = __popc(peers);
-            const int biggest = __reduce_max_sync(FULL, size);
-            const bool contiguous = peers == ((size == 32 ? FULL : ((1u << size) - 1u)) << head);
-            if (biggest >= 4 && __all_sync(FULL, contiguous)) {
-                const int last = head + size - 1;
-#pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-#pragma unroll
-                    for (int q = 0; q < SP; ++q) {
-                        const T other = __shfl_down_sync(FULL, acc[q], o);
-                        if (lane + o <= last) acc[q] += other;
-                    }
-                }
-                if (key >= 0 && lane == head) flush(key);
-            } else if (key >= 0) {
-                flush(key);
-            }
-            // the buffer is free, and the box complete, once every thread is past this point
             __syncthreads();
         }
-        m = e;
+        if (count == 0) break;
+        const int blo[3] = {s_step.blo[0], s_step.blo[1], s_step.blo[2]};
+        for (int j = t; j < count; j += kMaxBlock) {
+            const int q = (j / K) * PITCH + j % K;
+#pragma unroll
+            for (int d = 0; d < NDIM; ++d)
+                cp_async<sizeof(T)>(buf + d * ROW + q, a.pos + d * a.pos_stride + first + j);
+            cp_async<sizeof(T)>(buf + NDIM * ROW + q, a.values + first + j);
+        }
+        cp_async_commit();
+        cp_async_wait_all();
+        __syncthreads();
+        const int kq = (count + kMaxBlock - 1) / kMaxBlock;
+        const int j0 = t * kq;
+        const int nmine = min(kq, max(0, count - j0));
+        T acc[SP];
+#pragma unroll
+        for (int q = 0; q < SP; ++q) acc[q] = T(0);
+        int key = -1;  // the anchor of the open run, -1: none
+        // adds the open run to the box and empties it
+        auto flush = [&](int at) {
+#pragma unroll
+            for (int x = 0; x < S; ++x)
+#pragma unroll
+                for (int y = 0; y < SY; ++y)
+#pragma unroll
+                    for (int z = 0; z < SZ; ++z) {
+                        atomicAdd(box + at + x * sa + y * sb + z * se, acc[(x * SY + y) * SZ + z]);
+                        acc[(x * SY + y) * SZ + z] = T(0);
+                    }
+        };
+        // a run that ends: the plane of its window at the first node along the last axis is
+        // complete whatever comes next, and every ending run adds it in the same
+        // instructions; a run followed by the next cell along the last axis (anchor + 1)
+        // then slides its other planes down, any other adds them too and empties
+        constexpr int LASTN = NDIM == 3 ? SZ : (NDIM == 2 ? SY : S);
+        constexpr int OUTER = SP / LASTN;
+        auto end_run = [&](int at, bool adjacent) {
+#pragma unroll
+            for (int o = 0; o < OUTER; ++o) {
+                const int ob = NDIM == 3 ? (o / SY) * sa + (o % SY) * sb : (NDIM == 2 ? o * sa : 0);
+                atomicAdd(box + at + ob, acc[o * LASTN]);
+            }
+            if (adjacent) {
+#pragma unroll
+                for (int o = 0; o < OUTER; ++o) {
+#pragma unroll
+                    for (int l = 0; l + 1 < LASTN; ++l) acc[o * LASTN + l] = acc[o * LASTN + l + 1];
+                    acc[o * LASTN + LASTN - 1] = T(0);
+                }
+            } else {
+#pragma unroll
+                for (int o = 0; o < OUTER; ++o) {
+                    const int ob = NDIM == 3 ? (o / SY) * sa + (o % SY) * sb : (NDIM == 2 ? o * sa : 0);
+#pragma unroll
+                    for (int l = 1; l < LASTN; ++l) atomicAdd(box + at + ob + l, acc[o * LASTN + l]);
+                }
+#pragma unroll
+                for (int q = 0; q < SP; ++q) acc[q] = T(0);
+            }
+        };
+#pragma unroll 1
+        for (int s = 0; s < nmine; ++s) {
+            const int j = j0 + s;
+            const int q = (j / K) * PITCH + j % K;
+            const T v = buf[NDIM * ROW + q];
+            if (v == T(0)) continue;
+            T w[3][S];
+            int base[3] = {0, 0, 0};
+            int k = 0;
+            bool inside = true;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                if (d < NDIM) {
+                    const T rel = rel_from(buf[d * ROW + q], a.g, d);
+                    base[d] = axis_stencil<T, KIND, P>(rel, a.g.num[d], PERIODIC, w[d]);
+                    const int off = wrap_index(base[d] + H - blo[d], a.g.num[d]);
+                    inside = inside && (unsigned)off < (unsigned)tl[d];
+                    k += off * st[d];
+                } else {
+#pragma unroll
+                    for (int z = 0; z < S; ++z) w[d][z] = T(z == 0);
+                }
+            }
+            if (!inside) {  // not this tile's marker: straight to global memory
+                int64_t goff[3][S];
+                global_offsets<NDIM, S>(base, a.g.num, a.g.code, a.g.ext, goff);
+                const T vv[1] = {v};
+                stencil_add<T, NDIM, S, 1, int64_t>(a.field_out, goff, w, 1, 0, vv);
+                continue;
+            }
+            if (k != key && key >= 0) end_run(key, P > 0 && k == key + 1);
+            T wz[SZ];
+#pragma unroll
+            for (int z = 0; z < SZ; ++z) wz[z] = (NDIM > 2 ? w[2][z] : T(1)) * v;
+#pragma unroll
+            for (int x = 0; x < S; ++x)
+#pragma unroll
+                for (int y = 0; y < SY; ++y) {
+                    const T wxy = NDIM > 2 ? w[0][x] * w[1][y] : (NDIM > 1 ? w[0][x] * (w[1][y] * v) : w[0][x] * v);
+#pragma unroll
+                    for (int z = 0; z < SZ; ++z) {
+                        T& r = acc[(x * SY + y) * SZ + z];
+                        r = NDIM > 2 ? fma(wxy, wz[z], r) : r + wxy;
+                    }
+                }
+            key = k;
+        }
+        // the closing runs, as in the segment scatter
+        const int tag = key >= 0 ? key : -2 - lane;
+        const unsigned peers = __match_any_sync(FULL, tag);
+        const int head = __ffs(peers) - 1;
+        const int size = __popc(peers);
+        const int biggest = __reduce_max_sync(FULL, size);
+        const bool contiguous = peers == ((size == 32 ? FULL : ((1u << size) - 1u)) << head);
+        if (biggest >= 4 && __all_sync(FULL, contiguous)) {
+            const int last = head + size - 1;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+#pragma unroll
+                for (int q = 0; q < SP; ++q) {
+                    const T other = __shfl_down_sync(FULL, acc[q], o);
+                    if (lane + o <= last) acc[q] += other;
+                }
+            }
+            if (key >= 0 && lane == head) flush(key);
+        } else if (key >= 0) {
+            flush(key);
+        }
     }
-    retire(-1);
 }
 
 // The scatter. The markers of a chunk go to warps in contiguous runs of 32 (lane l of

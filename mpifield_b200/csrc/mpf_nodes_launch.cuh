@@ -133,9 +133,20 @@ static int run_scatter_tiles(NodeArgs<T> a, cudaStream_t stream) {
     const int smem = buf_bytes + (int)box_bytes;
     a.error = device_error_word();
     if (!a.error) return MPF_ERR_CUDA;
+    // the tile shapes of the 3D quadratic stores as compile-time constants, others at run time
     auto kernel = scatter_tiles_kernel<T, NDIM, KIND, P, K, MINB>;
-    static int cache[64] = {0};
-    if (allow_smem(kernel, smem, cache) != MPF_OK) return MPF_ERR_CUDA;
+    int shape = 0;
+    if constexpr (NDIM == 3 && P == 2) {
+        if (a.tile[0] == 8 && a.tile[1] == 8 && a.tile[2] == 8) {
+            kernel = scatter_tiles_kernel<T, NDIM, KIND, P, K, MINB, 8, 8, 8>;
+            shape = 1;
+        } else if (a.tile[0] == 8 && a.tile[1] == 8 && a.tile[2] == 16) {
+            kernel = scatter_tiles_kernel<T, NDIM, KIND, P, K, MINB, 8, 8, 16>;
+            shape = 2;
+        }
+    }
+    static int cache[3][64] = {{0}};
+    if (allow_smem(kernel, smem, cache[shape]) != MPF_OK) return MPF_ERR_CUDA;
     const int64_t units = (a.n + kMaxBlock - 1) / kMaxBlock;
     kernel<<<grid_for(units, smem, kMaxBlock, MINB), kMaxBlock, smem, stream>>>(a);
     count_launches(1);

@@ -77,7 +77,8 @@ def test_periodic_kinds_equal_the_oracle(ndim, kind, degree):
     assert _lib.device_errors() == 0
 
 
-@pytest.mark.parametrize("tile", [(1, 1, 1), (2, 3, 4), (8, 8, 8), (16, 16, 8), (24, 20, 18), (64, 64, 64)],
+@pytest.mark.parametrize("tile", [(1, 1, 1), (2, 3, 4), (8, 8, 8), (8, 8, 16), (16, 16, 8), (24, 20, 18),
+                                  (64, 64, 64)],
                          ids=lambda t: "x".join(map(str, t)))
 @pytest.mark.parametrize("within", [True, False], ids=["cells", "tiles"])
 def test_tile_shapes(tile, within):
@@ -86,6 +87,27 @@ def test_tile_shapes(tile, within):
     geom, ps, vs, order, ext = _store(rng, (24, 20, 18), (1, 1, 1), 60000, "quadratic", 2, tile, within)
     got = _scatter("quadratic", 2, ps, vs, ext, geom, order).cpu().numpy()
     assert rel_err(got, _oracle("quadratic", 2, ps, vs, ext, geom)) < RTOL_F64
+
+
+@pytest.mark.parametrize("kind", ["quadratic", "spline"])
+@pytest.mark.parametrize("tile", [(8, 8, 8), (8, 8, 16)], ids=lambda t: "x".join(map(str, t)))
+def test_compile_time_tile_shapes(kind, tile):
+    # the 3D degree-2 kernels with the tile shape as constants: uniform cells, a beam of
+    # dense cells, dead markers, rows of the last axis that end inside a thread's markers
+    rng = np.random.default_rng(sum(tile) + len(kind))
+    shape, cell, lower = (48, 40, 64), np.array([0.3, 0.2, 0.25]), np.array([-0.1, 0.2, -0.3])
+    span = cell * np.array(shape)
+    uniform = rng.uniform(0.0, 1.0, (150000, 3)) * span
+    beam = rng.normal(0.5, 0.02, (50000, 3)) * span
+    positions = (np.concatenate([uniform, beam]) + lower).T.copy()
+    values = rng.uniform(0.5, 1.5, (1, positions.shape[1]))
+    values[:, rng.uniform(size=positions.shape[1]) < 0.05] = 0.0
+    geom = (*lower, *cell, *shape, 1, 1, 1)
+    pos, val = torch.tensor(positions, device=DEV), torch.tensor(values, device=DEV)
+    order = mf.sort_by_tile(pos, (KIND_NAMES[kind], 2), geom, tile, values=val, within=True)
+    ps, vs = mf.permute(pos, order.order).contiguous(), mf.permute(val, order.order).contiguous()
+    got = _scatter(kind, 2, ps, vs, shape, geom, order).cpu().numpy()
+    assert rel_err(got, _oracle(kind, 2, ps, vs, shape, geom)) < RTOL_F64
 
 
 @pytest.mark.parametrize("shape", [(6, 5, 4), (12, 10, 8)], ids=["box_wider_than_grid", "one_tile"])
