@@ -535,12 +535,12 @@ def measure_fp32(step, ps, ws, reps: int) -> dict:
     p32, w32, f32 = ps.float(), ws.float(), step.field.float()
     E32 = torch.empty((3, n), dtype=torch.float32, device=ps.device)
     D32 = torch.zeros(step.density.shape, dtype=torch.float32, device=ps.device)
-    gather, scatter = mf.KERNELS["gather_quadratic_3d"], mf.KERNELS["scatter_quadratic_3d"]
+    gather = mf.KERNELS["gather_quadratic_3d"]
 
     def go():
         gather(p32, f32, E32, *step.geom)
         D32.zero_()
-        scatter(p32, w32, D32, *step.geom)
+        mf.kernels.scatter(step.lib.QUADRATIC, 2, p32, w32, D32, step.geom, order=step.order)
 
     ms = _event_ms(go, reps)
     err_e = float((E32.double() - E64).abs().max() / E64.abs().max())
