@@ -49,7 +49,7 @@ if str(ROOT) not in sys.path:
 
 METRIC = "markers/s: 3D quadratic gather/scatter"
 GRID = 256
-TILE = (8, 8, 16)
+TILE = (4, 4, 64)
 PEAK_FALLBACK_GBS = 6650.0
 
 

@@ -1085,30 +1085,38 @@ __global__ void __launch_bounds__(kMaxBlock, MINB) scatter_tiles_kernel(const No
         };
         // a run that ends: the plane of its window at the first node along the last axis is
         // complete whatever comes next, and every ending run adds it in the same
-        // instructions; a run followed by the next cell along the last axis (anchor + 1)
-        // then slides its other planes down, any other adds them too and empties
+        // instructions. A run followed by the next cell along the last axis (anchor + 1, the
+        // usual step in a store sorted by cell) slides its other planes down; one followed by
+        // the cell after that (anchor + 2: an empty cell between) adds its second plane too
+        // and slides by two; any other adds all of them and empties.
         constexpr int LASTN = NDIM == 3 ? SZ : (NDIM == 2 ? SY : S);
         constexpr int OUTER = SP / LASTN;
-        auto end_run = [&](int at, bool adjacent) {
+        auto end_run = [&](int at, int step) {
+            const int shift = (step >= 1 && step < LASTN) ? step : LASTN;
 #pragma unroll
-            for (int o = 0; o < OUTER; ++o) {
-                const int ob = NDIM == 3 ? (o / SY) * sa + (o % SY) * sb : (NDIM == 2 ? o * sa : 0);
-                atomicAdd(box + at + ob, acc[o * LASTN]);
+            for (int l = 0; l < LASTN; ++l) {
+                if (l == 0 || shift > l) {
+#pragma unroll
+                    for (int o = 0; o < OUTER; ++o) {
+                        const int ob = NDIM == 3 ? (o / SY) * sa + (o % SY) * sb : (NDIM == 2 ? o * sa : 0);
+                        atomicAdd(box + at + ob + l, acc[o * LASTN + l]);
+                    }
+                }
             }
-            if (adjacent) {
+            if (shift == 1) {
 #pragma unroll
                 for (int o = 0; o < OUTER; ++o) {
 #pragma unroll
                     for (int l = 0; l + 1 < LASTN; ++l) acc[o * LASTN + l] = acc[o * LASTN + l + 1];
                     acc[o * LASTN + LASTN - 1] = T(0);
                 }
-            } else {
+            } else if (LASTN > 2 && shift == 2) {
 #pragma unroll
                 for (int o = 0; o < OUTER; ++o) {
-                    const int ob = NDIM == 3 ? (o / SY) * sa + (o % SY) * sb : (NDIM == 2 ? o * sa : 0);
 #pragma unroll
-                    for (int l = 1; l < LASTN; ++l) atomicAdd(box + at + ob + l, acc[o * LASTN + l]);
+                    for (int l = 0; l < LASTN; ++l) acc[o * LASTN + l] = l + 2 < LASTN ? acc[o * LASTN + l + 2] : T(0);
                 }
+            } else {
 #pragma unroll
                 for (int q = 0; q < SP; ++q) acc[q] = T(0);
             }
@@ -1143,7 +1151,7 @@ __global__ void __launch_bounds__(kMaxBlock, MINB) scatter_tiles_kernel(const No
                 stencil_add<T, NDIM, S, 1, int64_t>(a.field_out, goff, w, 1, 0, vv);
                 continue;
             }
-            if (k != key && key >= 0) end_run(key, P > 0 && k == key + 1);
+            if (k != key && key >= 0) end_run(key, P > 0 ? k - key : 0);
             T wz[SZ];
 #pragma unroll
             for (int z = 0; z < SZ; ++z) wz[z] = (NDIM > 2 ? w[2][z] : T(1)) * v;

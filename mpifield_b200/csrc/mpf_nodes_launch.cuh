@@ -143,9 +143,12 @@ static int run_scatter_tiles(NodeArgs<T> a, cudaStream_t stream) {
         } else if (a.tile[0] == 8 && a.tile[1] == 8 && a.tile[2] == 16) {
             kernel = scatter_tiles_kernel<T, NDIM, KIND, P, K, MINB, 8, 8, 16>;
             shape = 2;
+        } else if (a.tile[0] == 4 && a.tile[1] == 4 && a.tile[2] == 64) {
+            kernel = scatter_tiles_kernel<T, NDIM, KIND, P, K, MINB, 4, 4, 64>;
+            shape = 3;
         }
     }
-    static int cache[3][64] = {{0}};
+    static int cache[4][64] = {{0}};
     if (allow_smem(kernel, smem, cache[shape]) != MPF_OK) return MPF_ERR_CUDA;
     const int64_t units = (a.n + kMaxBlock - 1) / kMaxBlock;
     kernel<<<grid_for(units, smem, kMaxBlock, MINB), kMaxBlock, smem, stream>>>(a);

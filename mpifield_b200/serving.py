@@ -236,18 +236,20 @@ def run_alone(req: Request, b: Buffers) -> torch.Tensor:
 
 def run_sorted(req: Request, b: Buffers) -> torch.Tensor:
     """A gather or scatter on its markers sorted by cell tile (8 cells a side), the sort's
-    buffers from the request's own; a gather's result goes back to the marker order."""
+    buffers from the request's own; a gather's result goes back to the marker order, a
+    scatter takes the sort's tile starts (the tile scatter)."""
     kind, degree = NODE_KIND[req.degree]
     geom = req.geometry
     scratch = iter([b["workspace"], b["keys"], b["order"], b["tile_start"]])
-    order = sort_by_tile(b["positions"], (kind, degree), geom, (8,) * req.ndim, within=True,
-                         alloc=lambda shape, dt: next(scratch)).order
-    pos = permute(b["positions"], order, out=b["sorted_positions"])
+    tiles = sort_by_tile(b["positions"], (kind, degree), geom, (8,) * req.ndim, within=True,
+                         alloc=lambda shape, dt: next(scratch))
+    pos = permute(b["positions"], tiles.order, out=b["sorted_positions"])
     if req.op == "gather":
         K.gather(kind, degree, pos, b["field"], b["sorted_out"], geom)
-        unpermute(b["sorted_out"], order, out=b["out"])
+        unpermute(b["sorted_out"], tiles.order, out=b["out"])
     else:
-        K.scatter(kind, degree, pos, permute(b["values"], order, out=b["sorted_values"]), b["out"], geom)
+        K.scatter(kind, degree, pos, permute(b["values"], tiles.order, out=b["sorted_values"]), b["out"], geom,
+                  order=tiles)
     return b["out"]
 
 

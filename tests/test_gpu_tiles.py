@@ -90,10 +90,11 @@ def test_tile_shapes(tile, within):
 
 
 @pytest.mark.parametrize("kind", ["quadratic", "spline"])
-@pytest.mark.parametrize("tile", [(8, 8, 8), (8, 8, 16)], ids=lambda t: "x".join(map(str, t)))
+@pytest.mark.parametrize("tile", [(8, 8, 8), (8, 8, 16), (4, 4, 64)], ids=lambda t: "x".join(map(str, t)))
 def test_compile_time_tile_shapes(kind, tile):
     # the 3D degree-2 kernels with the tile shape as constants: uniform cells, a beam of
-    # dense cells, dead markers, rows of the last axis that end inside a thread's markers
+    # dense cells, dead markers, rows of the last axis that end inside a thread's markers,
+    # empty cells inside a row (runs that end two cells apart)
     rng = np.random.default_rng(sum(tile) + len(kind))
     shape, cell, lower = (48, 40, 64), np.array([0.3, 0.2, 0.25]), np.array([-0.1, 0.2, -0.3])
     span = cell * np.array(shape)
