@@ -107,6 +107,22 @@ MPF_API int mpf_gather(int kind, int degree, int ndim, const void* positions, in
                int dtype, const mpf_tuning* tuning, void* stream);
 
 /*
+ * mpf_gather for markers sorted by cell tile: positions in the rank order of
+ * mpf_sort_by_tile (keys of the same kind, degree, geometry and `tile`), tile_start its
+ * num_tiles + 2 starts (8-byte aligned device memory). The result is mpf_gather's, bit for
+ * bit, whatever the order of the markers: a marker outside its rank's tile reads the field
+ * in global memory. With every axis periodic, 1-3 components and the tile's node box within
+ * a third of an SM's shared memory, each CTA copies a tile's box into shared memory once
+ * and its markers read it there; other shapes, and tuning->variant != 0, run mpf_gather's
+ * kernels. No counterpart in the reference (src/mpifield/weighting.py:233-250).
+ */
+MPF_API int mpf_gather_tiles(int kind, int degree, int ndim, const void* positions, int64_t pos_stride,
+                             int64_t n, const void* field, int64_t ncomp, void* result, int64_t res_stride,
+                             const double* lower, const double* cell, const int32_t* num,
+                             const int32_t* code, const int32_t* tile, const int64_t* tile_start,
+                             int dtype, const mpf_tuning* tuning, void* stream);
+
+/*
  * Node scatter (deposit): field(k, c) += sum_i W_k(x_i) values(c, i). A marker whose
  * values are all zero deposits nothing and its position is not read.
  * Replaces `scatter(positions, values, field, *geometry)`: scatter_{linear,quadratic,

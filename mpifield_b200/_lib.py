@@ -71,6 +71,7 @@ _SIGNATURES = {
     "mpf_status_string": ([_I], C.c_char_p),
     "mpf_gather": ([_I, _I, _I, _P, _L, _L, _P, _L, _P, _L, _P, _P, _P, _P, _I, _P, _P], _I),
     "mpf_scatter": ([_I, _I, _I, _P, _L, _P, _L, _L, _P, _L, _P, _P, _P, _P, _I, _P, _P], _I),
+    "mpf_gather_tiles": ([_I, _I, _I, _P, _L, _L, _P, _L, _P, _L, _P, _P, _P, _P, _P, _P, _I, _P, _P], _I),
     "mpf_scatter_tiles": ([_I, _I, _I, _P, _L, _P, _L, _L, _P, _L, _P, _P, _P, _P, _P, _P, _I, _P, _P], _I),
     "mpf_gather_grad": ([_I, _I, _I, _P, _L, _L, _P, _L, _P, _L, _P, _L, _P, _P, _P, _P, _I, _P], _I),
     "mpf_deposit_paths": ([_I, _I, _I, _P, _L, _P, _L, _P, _L, _P, _P, _P, _P, _P, _I, _P, _P], _I),

@@ -132,6 +132,18 @@ static NodeArgs<T> node_args(int ndim, int degree, const double* lower, const do
     return a;
 }
 
+// The tile-order fields of a launch (mpf_gather_tiles, mpf_scatter_tiles).
+template <typename T>
+static void set_tiles(NodeArgs<T>& a, int ndim, int degree, const int32_t* num, const int32_t* code,
+                      const int32_t* tile, const int64_t* tile_start, int64_t ntiles) {
+    a.tile_start = tile_start;
+    a.ntiles = ntiles;
+    for (int d = 0; d < ndim; ++d) {
+        a.tile[d] = tile[d];
+        a.tiles[d] = (int)((axis_extent(num[d], code[d], degree) + tile[d] - 1) / tile[d]);
+    }
+}
+
 }  // namespace mpf
 
 using namespace mpf;
@@ -207,6 +219,40 @@ int mpf_gather(int kind, int degree, int ndim, const void* positions, int64_t po
     return launch_gather<float>(kind, degree, ndim, a, t, s);
 }
 
+int mpf_gather_tiles(int kind, int degree, int ndim, const void* positions, int64_t pos_stride, int64_t n,
+                     const void* field, int64_t ncomp, void* result, int64_t res_stride, const double* lower,
+                     const double* cell, const int32_t* num, const int32_t* code, const int32_t* tile,
+                     const int64_t* tile_start, int dtype, const mpf_tuning* tuning, void* stream) {
+    if (!valid_kind(kind, degree) || (dtype != MPF_F64 && dtype != MPF_F32)) return MPF_ERR_ARGUMENT;
+    MPF_TRY(check_grid(kind, degree, ndim, lower, cell, num, code));
+    if (n < 0 || ncomp < 1 || ncomp > (1 << 20)) return MPF_ERR_ARGUMENT;
+    MPF_TRY(check_rows(positions, pos_stride, n, ndim, dtype));
+    MPF_TRY(check_rows(result, res_stride, n, (int)ncomp, dtype));
+    int64_t ntiles = 0;
+    MPF_TRY(mpf_num_tiles(kind, degree, ndim, num, code, tile, &ntiles));
+    if (!tile_start) return MPF_ERR_ARGUMENT;
+    if (reinterpret_cast<uintptr_t>(tile_start) % alignof(int64_t) != 0) return MPF_ERR_ALIGNMENT;
+    if (n == 0) return MPF_OK;
+    if (!field) return MPF_ERR_ARGUMENT;
+    if (!aligned(field, dtype)) return MPF_ERR_ALIGNMENT;
+    const Tuning t = tuning_of(tuning);
+    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (dtype == MPF_F64) {
+        NodeArgs<double> a = node_args<double>(ndim, degree, lower, cell, num, code);
+        a.pos = (const double*)positions; a.pos_stride = pos_stride;
+        a.field_in = (const double*)field; a.result = (double*)result; a.res_stride = res_stride;
+        a.n = n; a.ncomp = (int)ncomp;
+        set_tiles(a, ndim, degree, num, code, tile, tile_start, ntiles);
+        return launch_gather<double>(kind, degree, ndim, a, t, s);
+    }
+    NodeArgs<float> a = node_args<float>(ndim, degree, lower, cell, num, code);
+    a.pos = (const float*)positions; a.pos_stride = pos_stride;
+    a.field_in = (const float*)field; a.result = (float*)result; a.res_stride = res_stride;
+    a.n = n; a.ncomp = (int)ncomp;
+    set_tiles(a, ndim, degree, num, code, tile, tile_start, ntiles);
+    return launch_gather<float>(kind, degree, ndim, a, t, s);
+}
+
 int mpf_scatter(int kind, int degree, int ndim, const void* positions, int64_t pos_stride, const void* values,
                 int64_t val_stride, int64_t n, void* field, int64_t ncomp, const double* lower,
                 const double* cell, const int32_t* num, const int32_t* code, int dtype,
@@ -253,27 +299,19 @@ int mpf_scatter_tiles(int kind, int degree, int ndim, const void* positions, int
     if (!aligned(field, dtype)) return MPF_ERR_ALIGNMENT;
     const Tuning t = tuning_of(tuning);
     const cudaStream_t s = static_cast<cudaStream_t>(stream);
-    auto sorted = [&](auto& a) {
-        a.tile_start = tile_start;
-        a.ntiles = ntiles;
-        for (int d = 0; d < ndim; ++d) {
-            a.tile[d] = tile[d];
-            a.tiles[d] = (int)((axis_extent(num[d], code[d], degree) + tile[d] - 1) / tile[d]);
-        }
-    };
     if (dtype == MPF_F64) {
         NodeArgs<double> a = node_args<double>(ndim, degree, lower, cell, num, code);
         a.pos = (const double*)positions; a.pos_stride = pos_stride;
         a.values = (const double*)values; a.val_stride = val_stride;
         a.field_out = (double*)field; a.n = n; a.ncomp = (int)ncomp;
-        sorted(a);
+        set_tiles(a, ndim, degree, num, code, tile, tile_start, ntiles);
         return launch_scatter<double>(kind, degree, ndim, a, t, s);
     }
     NodeArgs<float> a = node_args<float>(ndim, degree, lower, cell, num, code);
     a.pos = (const float*)positions; a.pos_stride = pos_stride;
     a.values = (const float*)values; a.val_stride = val_stride;
     a.field_out = (float*)field; a.n = n; a.ncomp = (int)ncomp;
-    sorted(a);
+    set_tiles(a, ndim, degree, num, code, tile, tile_start, ntiles);
     return launch_scatter<float>(kind, degree, ndim, a, t, s);
 }
 

@@ -54,10 +54,59 @@ template <typename T, int NDIM> static int bulk_positions(const NodeArgs<T>& a) 
     return (p % 16 == 0) && (NDIM == 1 || (a.pos_stride * (int64_t)sizeof(T)) % 16 == 0) ? 1 : 0;
 }
 
-// Gather variants: 0 (default) through L1 while the field has fewer than 2^31 entries,
-// else with staged boxes; 1 staged boxes (path 1: global reads in that kernel); 2 through L1.
+// The tile gather (markers sorted by cell tile, periodic axes, 1-3 components): 256
+// threads, kGatherMinBlocks CTAs per SM. Returns MPF_ERR_ARGUMENT, launching nothing, when
+// the tile's node box does not fit that many CTAs' shared memory.
+template <typename T, int NDIM, int KIND, int P, int NC>
+static int run_gather_tiles(NodeArgs<T> a, cudaStream_t stream) {
+    constexpr int MINB = kGatherMinBlocks;
+    int64_t total = NC;
+    for (int d = 0; d < NDIM; ++d) {
+        int64_t e = (int64_t)a.tile[d] + P;
+        if (d == NDIM - 1 && (e & 1) == 0) ++e;
+        total *= e;
+    }
+    const int64_t box_bytes = total * (int64_t)sizeof(T);
+    if (box_bytes > (228 * 1024) / MINB - 2048) return MPF_ERR_ARGUMENT;
+    const int smem = (int)box_bytes;
+    a.error = device_error_word();
+    if (!a.error) return MPF_ERR_CUDA;
+    // the tile shapes of the 3D quadratic stores as compile-time constants, others at run time
+    auto kernel = gather_tiles_kernel<T, NDIM, KIND, P, NC, MINB>;
+    int shape = 0;
+    if constexpr (NDIM == 3 && P == 2) {
+        if (a.tile[0] == 8 && a.tile[1] == 8 && a.tile[2] == 8) {
+            kernel = gather_tiles_kernel<T, NDIM, KIND, P, NC, MINB, 8, 8, 8>;
+            shape = 1;
+        } else if (a.tile[0] == 8 && a.tile[1] == 8 && a.tile[2] == 16) {
+            kernel = gather_tiles_kernel<T, NDIM, KIND, P, NC, MINB, 8, 8, 16>;
+            shape = 2;
+        } else if (a.tile[0] == 4 && a.tile[1] == 4 && a.tile[2] == 64) {
+            kernel = gather_tiles_kernel<T, NDIM, KIND, P, NC, MINB, 4, 4, 64>;
+            shape = 3;
+        }
+    }
+    static int cache[4][64] = {{0}};
+    if (allow_smem(kernel, smem, cache[shape]) != MPF_OK) return MPF_ERR_CUDA;
+    const int64_t units = (a.n + kMaxBlock - 1) / kMaxBlock;
+    kernel<<<grid_for(units, smem, kMaxBlock, MINB), kMaxBlock, smem, stream>>>(a);
+    count_launches(1);
+    return launch_status();
+}
+
+// Gather variants: 0 (default) the tile gather for markers sorted by cell tile (periodic
+// axes, 1-3 components, the tile's node box within shared memory, fewer than 2^31 field
+// entries), else through L1 while the field has fewer than 2^31 entries, else with staged
+// boxes; 1 staged boxes (path 1: global reads in that kernel); 2 through L1.
 template <typename T, int NDIM, int KIND, int P, int NC>
 static int run_gather(NodeArgs<T> a, const Tuning& t, cudaStream_t stream) {
+    if constexpr (NC > 0) {
+        if (a.tile_start && t.variant == 0 && t.path != 1 && all_periodic<T, NDIM>(a) &&
+            field_entries<T, NDIM>(a) < ((int64_t)1 << 31)) {
+            const int st = run_gather_tiles<T, NDIM, KIND, P, NC>(a, stream);
+            if (st != MPF_ERR_ARGUMENT) return st;
+        }
+    }
     const bool l1 = t.variant != 1 && field_entries<T, NDIM>(a) < ((int64_t)1 << 31);
     const int block = l1 ? kMaxBlock : pick_block(t);
     const int CH = kMarkersPerThread * block;

@@ -106,9 +106,23 @@ class NodeKernel:
             scatter(self.kind, degree, positions, values, field, geometry, self.tuning)
 
 
+def _tile_args(order, ndim: int, device):
+    """The tile shape (ctypes array) and tile starts of a `sorting.TileOrder`, checked."""
+    starts = order.tile_start
+    if starts.device != device or starts.dtype != torch.int64 or not starts.is_contiguous():
+        raise ValueError("order.tile_start must be a contiguous int64 tensor on the markers' device")
+    if len(order.tile) != ndim or starts.numel() != order.num_tiles + 2:
+        raise ValueError(f"a tile order of {len(order.tile)} axes and {starts.numel()} starts for a {ndim}D grid")
+    return (C.c_int32 * ndim)(*(int(v) for v in order.tile)), starts.data_ptr()
+
+
 def gather(kind: int, degree: int, positions: torch.Tensor, field: torch.Tensor, result: torch.Tensor,
-           geometry, tuning: _lib.Tuning | None = None) -> None:
-    """result(c, i) = sum_k W_k(x_i) field(k, c), overwriting ``result`` (ncomp, N)."""
+           geometry, tuning: _lib.Tuning | None = None, order=None) -> None:
+    """result(c, i) = sum_k W_k(x_i) field(k, c), overwriting ``result`` (ncomp, N).
+
+    ``order``: the `sorting.TileOrder` whose rank order the markers are in, for
+    ``mpf_gather_tiles`` (the same result, whatever the markers' order).
+    """
     lower, cell, num, code, ndim = _lib.geometry_arrays(geometry)
     device = _lib.require_cuda(positions, field, result)
     dtype = field.dtype
@@ -126,10 +140,16 @@ def gather(kind: int, degree: int, positions: torch.Tensor, field: torch.Tensor,
     rows_ok = result.dtype == dtype and (n <= 1 or result.stride(1) == 1) and (ncomp == 1 or result.stride(0) >= n)
     out = result if rows_ok else torch.empty((ncomp, n), dtype=dtype, device=device)
     rs = out.stride(0) if ncomp > 1 else n
-    status = _lib.library().mpf_gather(
-        kind, degree, ndim, pos.data_ptr(), ps, n, field.data_ptr(), ncomp, out.data_ptr(), rs,
-        lower, cell, num, code, dcode, C.byref(tuning) if tuning is not None else None,
-        _lib.stream_of(device))
+    tune = C.byref(tuning) if tuning is not None else None
+    if order is None:
+        status = _lib.library().mpf_gather(
+            kind, degree, ndim, pos.data_ptr(), ps, n, field.data_ptr(), ncomp, out.data_ptr(), rs,
+            lower, cell, num, code, dcode, tune, _lib.stream_of(device))
+    else:
+        tile, starts = _tile_args(order, ndim, device)
+        status = _lib.library().mpf_gather_tiles(
+            kind, degree, ndim, pos.data_ptr(), ps, n, field.data_ptr(), ncomp, out.data_ptr(), rs,
+            lower, cell, num, code, tile, starts, dcode, tune, _lib.stream_of(device))
     _lib.check(status, "gather")
     if out is not result:
         result.copy_(out)
@@ -160,16 +180,10 @@ def scatter(kind: int, degree: int, positions: torch.Tensor, values: torch.Tenso
             kind, degree, ndim, pos.data_ptr(), ps, vals.data_ptr(), vs, pos.shape[1], out.work.data_ptr(),
             ncomp, lower, cell, num, code, dcode, tune, _lib.stream_of(device))
     else:
-        starts = order.tile_start
-        if starts.device != device or starts.dtype != torch.int64 or not starts.is_contiguous():
-            raise ValueError("order.tile_start must be a contiguous int64 tensor on the markers' device")
-        if len(order.tile) != ndim or starts.numel() != order.num_tiles + 2:
-            raise ValueError(f"a tile order of {len(order.tile)} axes and {starts.numel()} starts "
-                             f"for a {ndim}D grid")
-        tile = (C.c_int32 * ndim)(*(int(v) for v in order.tile))
+        tile, starts = _tile_args(order, ndim, device)
         status = _lib.library().mpf_scatter_tiles(
             kind, degree, ndim, pos.data_ptr(), ps, vals.data_ptr(), vs, pos.shape[1], out.work.data_ptr(),
-            ncomp, lower, cell, num, code, tile, starts.data_ptr(), dcode, tune, _lib.stream_of(device))
+            ncomp, lower, cell, num, code, tile, starts, dcode, tune, _lib.stream_of(device))
     _lib.check(status, "scatter")
     out.finish()
 

@@ -236,8 +236,8 @@ def run_alone(req: Request, b: Buffers) -> torch.Tensor:
 
 def run_sorted(req: Request, b: Buffers) -> torch.Tensor:
     """A gather or scatter on its markers sorted by cell tile (8 cells a side), the sort's
-    buffers from the request's own; a gather's result goes back to the marker order, a
-    scatter takes the sort's tile starts (the tile scatter)."""
+    buffers from the request's own, the kernels given the sort's tile starts (the tile
+    gather and scatter); a gather's result goes back to the marker order."""
     kind, degree = NODE_KIND[req.degree]
     geom = req.geometry
     scratch = iter([b["workspace"], b["keys"], b["order"], b["tile_start"]])
@@ -245,7 +245,7 @@ def run_sorted(req: Request, b: Buffers) -> torch.Tensor:
                          alloc=lambda shape, dt: next(scratch))
     pos = permute(b["positions"], tiles.order, out=b["sorted_positions"])
     if req.op == "gather":
-        K.gather(kind, degree, pos, b["field"], b["sorted_out"], geom)
+        K.gather(kind, degree, pos, b["field"], b["sorted_out"], geom, order=tiles)
         unpermute(b["sorted_out"], tiles.order, out=b["out"])
     else:
         K.scatter(kind, degree, pos, permute(b["values"], tiles.order, out=b["sorted_values"]), b["out"], geom,

@@ -1,4 +1,4 @@
-"""GPU parity of the tile scatter (mpf_scatter_tiles) with the oracle.
+"""GPU parity of the tile scatter and gather (mpf_scatter_tiles, mpf_gather_tiles) with the oracle.
 
 Markers sorted by cell tile (mpf_sort_by_tile) and permuted into rank order are
 scattered with the sort's tile starts; FP64 results agree with the oracle's scatter of
@@ -9,7 +9,9 @@ scatter), tiles sorted with and without the cell inside the tile, dead markers i
 sentinel tile, dense cells split across CTAs, a store whose tile starts do not belong
 to its positions (every marker outside its rank's tile adds to global memory), bounded
 and clamped axes (the segment scatter), several components, FP32, and at 2^24 markers
-the size-independent property: the tile scatter equals mpf_scatter on the same store.
+the size-independent property: the tile scatter equals mpf_scatter on the same store. The
+tile gather equals mpf_gather bit for bit (the same sums in the same order) on the same
+shapes, tiles and stores, and the oracle within RTOL_F64.
 """
 
 from __future__ import annotations
@@ -20,7 +22,7 @@ import torch
 
 import mpifield_b200 as mf
 from mpifield_b200 import _lib
-from mpifield_b200.kernels import scatter
+from mpifield_b200.kernels import gather, scatter
 from oracle import oracle as O
 from tests.helpers import KIND_NAMES, RTOL_F32, RTOL_F64, rel_err
 
@@ -220,3 +222,88 @@ def test_bad_tile_orders_are_refused():
     bad = mf.TileOrder(order.keys, order.order, order.tile_start, order.num_tiles, (8, 8))
     with pytest.raises(ValueError):
         scatter(KIND_NAMES["quadratic"], 2, ps, vs, field, geom, order=bad)
+
+
+# ------------------------------------------------------------------ the tile gather --
+
+def _gather_pair(kind, degree, ps, field, geom, order):
+    ncomp = field.shape[-1]
+    tiles = torch.empty((ncomp, ps.shape[1]), dtype=ps.dtype, device=DEV)
+    plain = torch.empty_like(tiles)
+    gather(KIND_NAMES[kind], degree, ps, field, tiles, geom, order=order)
+    gather(KIND_NAMES[kind], degree, ps, field, plain, geom)
+    return tiles, plain
+
+
+@pytest.mark.parametrize("ndim", [1, 2, 3])
+@pytest.mark.parametrize("kind,degree", KINDS, ids=[f"{k}{d}" for k, d in KINDS])
+def test_tile_gather_equals_the_gather_bit_for_bit(ndim, kind, degree):
+    rng = np.random.default_rng(100 + 10 * ndim + degree)
+    shape = (40, 24, 18)[:ndim]
+    tile = (8, 6, 5)[:ndim]
+    geom, ps, _, order, ext = _store(rng, shape, (1,) * ndim, 20000, kind, degree, tile)
+    field = torch.tensor(rng.normal(size=ext + (3,)), device=DEV)
+    tiles, plain = _gather_pair(kind, degree, ps, field, geom, order)
+    assert torch.equal(tiles, plain)
+    oracle = O.gather(kind, degree, ps.cpu().numpy(), field.cpu().numpy(), geom)
+    assert rel_err(tiles.cpu().numpy(), oracle) < RTOL_F64
+
+
+@pytest.mark.parametrize("tile", [(1, 1, 1), (8, 8, 8), (8, 8, 16), (4, 4, 64), (16, 16, 8), (64, 64, 64)],
+                         ids=lambda t: "x".join(map(str, t)))
+@pytest.mark.parametrize("ncomp", [1, 2, 3, 5])
+def test_tile_gather_shapes_and_components(tile, ncomp):
+    # 64^3 tiles do not fit shared memory and 5 components take the L1 gather
+    rng = np.random.default_rng(sum(tile) + ncomp)
+    geom, ps, _, order, ext = _store(rng, (24, 20, 70), (1, 1, 1), 60000, "quadratic", 2, tile)
+    field = torch.tensor(rng.normal(size=ext + (ncomp,)), device=DEV)
+    tiles, plain = _gather_pair("quadratic", 2, ps, field, geom, order)
+    assert torch.equal(tiles, plain)
+
+
+def test_tile_gather_with_the_tile_starts_of_another_store():
+    rng = np.random.default_rng(21)
+    geom, ps, _, order, ext = _store(rng, (30, 26, 22), (1, 1, 1), 40000, "quadratic", 2, (8, 8, 8))
+    perm = torch.randperm(ps.shape[1], generator=torch.Generator().manual_seed(1)).to(DEV)
+    ps2 = ps[:, perm].contiguous()
+    field = torch.tensor(rng.normal(size=ext + (3,)), device=DEV)
+    tiles, plain = _gather_pair("quadratic", 2, ps2, field, geom, order)
+    assert torch.equal(tiles, plain)
+
+
+@pytest.mark.parametrize("codes", [(0, 0, 0), (2, 1, 1)], ids=["bounded", "clamped"])
+def test_tile_gather_other_boundaries(codes):
+    rng = np.random.default_rng(22)
+    geom, ps, _, order, ext = _store(rng, (20, 18, 16), codes, 30000, "spline", 2, (8, 8, 8))
+    field = torch.tensor(rng.normal(size=ext + (3,)), device=DEV)
+    tiles, plain = _gather_pair("spline", 2, ps, field, geom, order)
+    assert torch.equal(tiles, plain)
+
+
+def test_tile_gather_float32_and_a_beam():
+    rng = np.random.default_rng(23)
+    shape = (48, 40, 64)
+    beam = rng.normal(0.5, 0.02, (3, 80000)) * np.array(shape)[:, None]
+    geom = (0.0, 0.0, 0.0, 1.0, 1.0, 1.0, *shape, 1, 1, 1)
+    for dtype in (torch.float64, torch.float32):
+        pos = torch.tensor(np.concatenate([beam, rng.uniform(0, 1, (3, 20000)) * np.array(shape)[:, None]], 1),
+                           dtype=dtype, device=DEV)
+        order = mf.sort_by_tile(pos, mf.QUADRATIC, geom, (4, 4, 64), within=True)
+        ps = mf.permute(pos, order.order).contiguous()
+        field = torch.tensor(rng.normal(size=shape + (3,)), dtype=dtype, device=DEV)
+        tiles, plain = _gather_pair("quadratic", 2, ps, field, geom, order)
+        assert torch.equal(tiles, plain)
+    assert _lib.device_errors() == 0
+
+
+def test_the_tile_gather_equals_the_gather_at_2_24_markers():
+    n, grid = 1 << 24, 160
+    g = torch.Generator(device=DEV).manual_seed(24)
+    geom = (0.0, 0.0, 0.0, 1 / grid, 1 / grid, 1 / grid, grid, grid, grid, 1, 1, 1)
+    pos = torch.rand((3, n), generator=g, dtype=torch.float64, device=DEV)
+    order = mf.sort_by_tile(pos, mf.QUADRATIC, geom, (4, 4, 64), within=True)
+    ps = mf.permute(pos, order.order).contiguous()
+    del pos
+    field = torch.randn((grid, grid, grid, 3), generator=g, dtype=torch.float64, device=DEV)
+    tiles, plain = _gather_pair("quadratic", 2, ps, field, geom, order)
+    assert torch.equal(tiles, plain)
