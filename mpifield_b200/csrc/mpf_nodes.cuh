@@ -36,6 +36,9 @@ constexpr int kGatherMinBlocks = 3;
 // Consecutive markers per thread in the segment scatter, and the widest margin of its boxes.
 constexpr int kSegment = 8;
 constexpr int kScatterMargin = 0;
+// The tile scatter's CTA: threads and resident CTAs per SM (128 registers a thread).
+constexpr int kTileScatterBlock = 256;
+constexpr int kTileScatterMinBlocks = 2;
 
 template <typename T>
 __device__ __forceinline__ T rel_of(const NodeArgs<T>& a, int d, int64_t i) {
@@ -924,10 +927,11 @@ __device__ __forceinline__ void flush_clear_box(T* box, T* field, const int* lo,
 // tiles before the sentinel) splits at tile boundaries into pieces whose box is known
 // in advance: the tile's anchors widened by the stencil, tile + P nodes per axis (the
 // last axis made odd for the shared-memory banks). No box reduction, no frame choice,
-// one flush per piece, fused with the zeroing. A piece is cut into nearly equal
-// sub-chunks of at most 256 x K markers, thread t owning the contiguous markers
-// t kq .. t kq + kq - 1 (kq = ceil(count / 256)) in the padded rows of the segment
-// scatter. Runs of one anchor are summed in registers and added to the box as there,
+// one flush per piece, fused with the zeroing. Thread t owns the t-th of 256 contiguous
+// ranges of a piece, taken K markers at a time in sub-chunks (the padded rows of the
+// segment scatter, thread t's markers at t (K + 1) ..), so a thread's runs carry over the
+// sub-chunk boundaries and close once per piece. Runs of one anchor are summed in
+// registers and added to the box as there,
 // except that a run followed by the next cell along the last axis (anchor + 1, the
 // usual step in a store sorted by cell) adds only the plane of its window that the
 // next run does not touch and slides the rest: S^(NDIM-1) shared-memory atomics
@@ -944,16 +948,20 @@ struct TileLoop {
     int sub, nsub;     // sub-chunks of the current piece: done, in all
 };
 struct TileStep {
-    int64_t first;  // the sub-chunk's first rank
-    int count;      // its markers (0: the CTA is done)
+    int64_t first;  // the sub-chunk's first rank (with thread ranges: the piece's)
+    int count;      // its markers (with thread ranges: the piece's; 0: the CTA is done)
+    int sub, nsub;  // with thread ranges: the sub-chunk of the piece, and their number
     int retire;     // 1: add the box of the previous tile (first node old_lo) to the field first
     int blo[3];     // the sub-chunk's tile: its first anchor per axis
     int old_lo[3];
 };
 
-// Thread 0's plan of the next sub-chunk (tile pieces cut at tile_start, each into nearly
-// equal sub-chunks of at most ch markers).
-template <int NDIM, int H>
+// Thread 0's plan of the next sub-chunk: tile pieces cut at tile_start (at most 2^30
+// markers), each into nearly equal sub-chunks of at most ch markers, or with thread ranges
+// (RANGES: the piece's markers split into blockDim.x contiguous ranges, sub-chunk s taking
+// markers s ch .. s ch + ch - 1 of every range) into as many sub-chunks as the longest
+// range needs.
+template <int NDIM, int H, bool RANGES = false>
 __device__ __forceinline__ void plan_tile_step(TileLoop& L, TileStep& st, const int64_t* ts, int64_t ntiles,
                                                const int* tiles, const int* tl, int ch) {
     st.retire = 0;
@@ -968,7 +976,7 @@ __device__ __forceinline__ void plan_tile_step(TileLoop& L, TileStep& st, const 
             return;
         }
         const int64_t tt = tile_of(ts, ntiles, L.cur, L.m);
-        L.e = min(L.m_end, max(L.m + 1, __ldg(ts + tt + 1)));
+        L.e = min(min(L.m_end, L.m + ((int64_t)1 << 30)), max(L.m + 1, __ldg(ts + tt + 1)));
         if (tt != L.cur) {
             st.retire = L.cur >= 0 ? 1 : 0;
             int rest = (int)tt;  // tiles number fewer than 2^31
@@ -981,34 +989,39 @@ __device__ __forceinline__ void plan_tile_step(TileLoop& L, TileStep& st, const 
             }
             L.cur = tt;
         }
-        const int64_t len = L.e - L.m;
-        if (len < ((int64_t)1 << 31)) {  // 32-bit divisions for the usual piece
-            const int n32 = (int)len;
+        const int n32 = (int)(L.e - L.m);  // below 2^30
+        if (RANGES) {
+            const int longest = n32 / (int)blockDim.x + (n32 % (int)blockDim.x != 0 ? 1 : 0);
+            L.nsub = longest / ch + (longest % ch != 0 ? 1 : 0);
+        } else {
             L.nsub = n32 / ch + (n32 % ch != 0 ? 1 : 0);
             L.part = n32 / L.nsub;
             L.extra = n32 - (int)L.part * L.nsub;
-        } else {
-            L.nsub = (int)((len + ch - 1) / ch);
-            L.part = len / L.nsub;
-            L.extra = len % L.nsub;
         }
         L.sub = 0;
     }
-    st.first = L.m + L.sub * L.part + min((int64_t)L.sub, L.extra);
-    st.count = (int)(L.part + (L.sub < L.extra ? 1 : 0));
+    if (RANGES) {
+        st.first = L.m;
+        st.count = (int)(L.e - L.m);
+    } else {
+        st.first = L.m + L.sub * L.part + min((int64_t)L.sub, L.extra);
+        st.count = (int)(L.part + (L.sub < L.extra ? 1 : 0));
+    }
+    st.sub = L.sub;
+    st.nsub = L.nsub;
     ++L.sub;
 }
 
-template <typename T, int NDIM, int KIND, int P, int K, int MINB, int TX = 0, int TY = 0, int TZ = 0>
-__global__ void __launch_bounds__(kMaxBlock, MINB) scatter_tiles_kernel(const NodeArgs<T> a) {
+template <typename T, int NDIM, int KIND, int P, int K, int MINB, int TX = 0, int TY = 0, int TZ = 0,
+          int BLOCK = kMaxBlock>
+__global__ void __launch_bounds__(BLOCK, MINB) scatter_tiles_kernel(const NodeArgs<T> a) {
     constexpr int S = P + 1;
     constexpr int SY = NDIM > 1 ? S : 1;
     constexpr int SZ = NDIM > 2 ? S : 1;
     constexpr int SP = S * SY * SZ;
     constexpr int PITCH = K + 1;
     constexpr int ROWS = NDIM + 1;
-    constexpr int CH = kMaxBlock * K;
-    constexpr int ROW = kMaxBlock * PITCH;
+    constexpr int ROW = BLOCK * PITCH;
     constexpr int H = P / 2;  // a stencil's anchor is its first node + H
     constexpr unsigned FULL = 0xffffffffu;
     __shared__ TileLoop s_loop;
@@ -1022,7 +1035,7 @@ __global__ void __launch_bounds__(kMaxBlock, MINB) scatter_tiles_kernel(const No
     const int tl[3] = {TX > 0 ? TX : a.tile[0], TY > 0 ? TY : a.tile[1], TZ > 0 ? TZ : a.tile[2]};
     int ex[3] = {1, 1, 1};
     tile_box_extents<NDIM, P>(tl, ex);
-    for (int q = t; q < ex[0] * ex[1] * ex[2]; q += kMaxBlock) box[q] = T(0);
+    for (int q = t; q < ex[0] * ex[1] * ex[2]; q += BLOCK) box[q] = T(0);
     if (t == 0) {
         const int64_t live = min(max(__ldg(a.tile_start + a.ntiles), (int64_t)0), a.n);
         const int64_t per = (live + gridDim.x - 1) / gridDim.x;
@@ -1040,13 +1053,20 @@ __global__ void __launch_bounds__(kMaxBlock, MINB) scatter_tiles_kernel(const No
     const int sb = NDIM > 2 ? ex[2] : (NDIM > 1 ? 1 : 0);
     const int sa = NDIM > 2 ? ex[1] * ex[2] : (NDIM > 1 ? ex[1] : 1);
     const int st[3] = {sa, NDIM > 1 ? sb : 0, NDIM > 2 ? se : 0};
+    // the open run of the thread: it carries over the sub-chunks of a piece
+    T acc[SP];
+#pragma unroll
+    for (int q = 0; q < SP; ++q) acc[q] = T(0);
+    int key = -1;  // the anchor of the open run, -1: none
 #pragma unroll 1
     for (;;) {
-        if (t == 0) plan_tile_step<NDIM, H>(s_loop, s_step, a.tile_start, a.ntiles, a.tiles, tl, CH);
+        if (t == 0) plan_tile_step<NDIM, H, true>(s_loop, s_step, a.tile_start, a.ntiles, a.tiles, tl, K);
         // the plan is visible, the previous sub-chunk's adds are complete and its rows free
         __syncthreads();
         const int64_t first = s_step.first;
         const int count = s_step.count;
+        const int sub = s_step.sub;
+        const bool closing = sub + 1 >= s_step.nsub;
         if (s_step.retire) {
             const int lo[3] = {s_step.old_lo[0], s_step.old_lo[1], s_step.old_lo[2]};
             flush_clear_box<T, NDIM>(box, a.field_out, lo, ex, a.g);
@@ -1054,23 +1074,26 @@ __global__ void __launch_bounds__(kMaxBlock, MINB) scatter_tiles_kernel(const No
         }
         if (count == 0) break;
         const int blo[3] = {s_step.blo[0], s_step.blo[1], s_step.blo[2]};
-        for (int j = t; j < count; j += kMaxBlock) {
-            const int q = (j / K) * PITCH + j % K;
+        // the piece in BLOCK contiguous ranges (thread u: `per` markers, one more for
+        // u < rem); this sub-chunk holds markers sub K .. sub K + K - 1 of every range,
+        // thread u's at row position u (K + 1) + j, read by groups of K consecutive lanes
+        const int per = count / BLOCK, rem = count % BLOCK;
+        for (int q = t; q < BLOCK * K; q += BLOCK) {
+            const int u = q / K, j = q % K;
+            const int idx = sub * K + j;
+            if (idx < per + (u < rem ? 1 : 0)) {
+                const int64_t g = first + (int64_t)u * per + min(u, rem) + idx;
+                const int at = u * PITCH + j;
 #pragma unroll
-            for (int d = 0; d < NDIM; ++d)
-                cp_async<sizeof(T)>(buf + d * ROW + q, a.pos + d * a.pos_stride + first + j);
-            cp_async<sizeof(T)>(buf + NDIM * ROW + q, a.values + first + j);
+                for (int d = 0; d < NDIM; ++d)
+                    cp_async<sizeof(T)>(buf + d * ROW + at, a.pos + d * a.pos_stride + g);
+                cp_async<sizeof(T)>(buf + NDIM * ROW + at, a.values + g);
+            }
         }
         cp_async_commit();
         cp_async_wait_all();
         __syncthreads();
-        const int kq = (count + kMaxBlock - 1) / kMaxBlock;
-        const int j0 = t * kq;
-        const int nmine = min(kq, max(0, count - j0));
-        T acc[SP];
-#pragma unroll
-        for (int q = 0; q < SP; ++q) acc[q] = T(0);
-        int key = -1;  // the anchor of the open run, -1: none
+        const int nmine = min(K, max(0, per + (t < rem ? 1 : 0) - sub * K));
         // adds the open run to the box and empties it
         auto flush = [&](int at) {
 #pragma unroll
@@ -1123,8 +1146,7 @@ __global__ void __launch_bounds__(kMaxBlock, MINB) scatter_tiles_kernel(const No
         };
 #pragma unroll 1
         for (int s = 0; s < nmine; ++s) {
-            const int j = j0 + s;
-            const int q = (j / K) * PITCH + j % K;
+            const int q = t * PITCH + s;
             const T v = buf[NDIM * ROW + q];
             if (v == T(0)) continue;
             T w[3][S];
@@ -1168,6 +1190,7 @@ __global__ void __launch_bounds__(kMaxBlock, MINB) scatter_tiles_kernel(const No
                 }
             key = k;
         }
+        if (!closing) continue;  // the runs go on in the piece's next sub-chunk
         // the closing runs, as in the segment scatter
         const int tag = key >= 0 ? key : -2 - lane;
         const unsigned peers = __match_any_sync(FULL, tag);
@@ -1189,6 +1212,10 @@ __global__ void __launch_bounds__(kMaxBlock, MINB) scatter_tiles_kernel(const No
         } else if (key >= 0) {
             flush(key);
         }
+        // every run is closed (the other lanes of a group summed into its head)
+#pragma unroll
+        for (int q = 0; q < SP; ++q) acc[q] = T(0);
+        key = -1;
     }
 }
 

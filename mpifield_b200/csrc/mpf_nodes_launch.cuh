@@ -165,12 +165,12 @@ static int run_scatter_segments(NodeArgs<T> a, const Tuning& t, cudaStream_t str
     return launch_status();
 }
 
-// The tile scatter (markers sorted by cell tile, one component, periodic axes): 256
+// The tile scatter (markers sorted by cell tile, one component, periodic axes): BLOCK
 // threads, MINB CTAs per SM, each CTA an equal share of the live markers. Returns
 // MPF_ERR_ARGUMENT, launching nothing, when the tile's box does not fit beside the rows.
-template <typename T, int NDIM, int KIND, int P, int K, int MINB>
+template <typename T, int NDIM, int KIND, int P, int K, int MINB, int BLOCK>
 static int run_scatter_tiles(NodeArgs<T> a, cudaStream_t stream) {
-    const int buf_bytes = (NDIM + 1) * kMaxBlock * (K + 1) * (int)sizeof(T);
+    const int buf_bytes = (NDIM + 1) * BLOCK * (K + 1) * (int)sizeof(T);
     int64_t total = 1;
     for (int d = 0; d < NDIM; ++d) {
         int64_t e = (int64_t)a.tile[d] + P;
@@ -183,24 +183,24 @@ static int run_scatter_tiles(NodeArgs<T> a, cudaStream_t stream) {
     a.error = device_error_word();
     if (!a.error) return MPF_ERR_CUDA;
     // the tile shapes of the 3D quadratic stores as compile-time constants, others at run time
-    auto kernel = scatter_tiles_kernel<T, NDIM, KIND, P, K, MINB>;
+    auto kernel = scatter_tiles_kernel<T, NDIM, KIND, P, K, MINB, 0, 0, 0, BLOCK>;
     int shape = 0;
     if constexpr (NDIM == 3 && P == 2) {
         if (a.tile[0] == 8 && a.tile[1] == 8 && a.tile[2] == 8) {
-            kernel = scatter_tiles_kernel<T, NDIM, KIND, P, K, MINB, 8, 8, 8>;
+            kernel = scatter_tiles_kernel<T, NDIM, KIND, P, K, MINB, 8, 8, 8, BLOCK>;
             shape = 1;
         } else if (a.tile[0] == 8 && a.tile[1] == 8 && a.tile[2] == 16) {
-            kernel = scatter_tiles_kernel<T, NDIM, KIND, P, K, MINB, 8, 8, 16>;
+            kernel = scatter_tiles_kernel<T, NDIM, KIND, P, K, MINB, 8, 8, 16, BLOCK>;
             shape = 2;
         } else if (a.tile[0] == 4 && a.tile[1] == 4 && a.tile[2] == 64) {
-            kernel = scatter_tiles_kernel<T, NDIM, KIND, P, K, MINB, 4, 4, 64>;
+            kernel = scatter_tiles_kernel<T, NDIM, KIND, P, K, MINB, 4, 4, 64, BLOCK>;
             shape = 3;
         }
     }
     static int cache[4][64] = {{0}};
     if (allow_smem(kernel, smem, cache[shape]) != MPF_OK) return MPF_ERR_CUDA;
-    const int64_t units = (a.n + kMaxBlock - 1) / kMaxBlock;
-    kernel<<<grid_for(units, smem, kMaxBlock, MINB), kMaxBlock, smem, stream>>>(a);
+    const int64_t units = (a.n + BLOCK - 1) / BLOCK;
+    kernel<<<grid_for(units, smem, BLOCK, MINB), BLOCK, smem, stream>>>(a);
     count_launches(1);
     return launch_status();
 }
@@ -215,7 +215,7 @@ static int run_scatter(NodeArgs<T> a, const Tuning& t, cudaStream_t stream) {
     constexpr int SP = StencilPoints<P + 1, NDIM>::value;
     if constexpr (NC == 1 && SP <= 27) {
         if (a.tile_start && t.variant == 0 && t.path != 1 && all_periodic<T, NDIM>(a)) {
-            const int st = run_scatter_tiles<T, NDIM, KIND, P, kSegment, 2>(a, stream);
+            const int st = run_scatter_tiles<T, NDIM, KIND, P, kSegment, kTileScatterMinBlocks, kTileScatterBlock>(a, stream);
             if (st != MPF_ERR_ARGUMENT) return st;
         }
         if (t.variant == 3) return run_scatter_segments<T, NDIM, KIND, P, 4, 3>(a, t, stream);
