@@ -56,7 +56,7 @@ PEAK_FALLBACK_GBS = 6650.0
 def parse() -> argparse.Namespace:
     p = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--steps", type=int, default=40)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=("ours", "reference"), default="ours")
     p.add_argument("--markers", type=int, default=1 << 26)
@@ -134,10 +134,15 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits", "-lms", "200",
+                ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits", "-lms", "20",
                  "-i", str(self.index)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            # the timed region starts once the sampler is live (its first line is out)
+            deadline = time.perf_counter() + 3.0
+            while not self.lines and self.proc.poll() is None and time.perf_counter() < deadline:
+                time.sleep(0.005)
+            self.skip = len(self.lines)
         except (FileNotFoundError, OSError):
             self.proc = None
         return self
@@ -155,7 +160,7 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self) -> dict | None:
-        rows = [line.split(", ") for line in self.lines if line.count(",") >= 8]
+        rows = [line.split(", ") for line in self.lines[getattr(self, "skip", 0):] if line.count(",") >= 8]
         if not rows:
             return None
         sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
