@@ -602,6 +602,85 @@ __global__ void __launch_bounds__(kMaxBlock, MINB) gather_l1_kernel(const NodeAr
     }
 }
 
+// ------------------------------------------------- runs of one stencil anchor --
+//
+// The open run of a thread in the segment and tile scatters: the weighted sums of its
+// markers of one anchor, acc[(x SY + y) SZ + z] for node (x, y, z) of the stencil.
+
+template <int NDIM, int S> struct RunShape {
+    static constexpr int SY = NDIM > 1 ? S : 1;
+    static constexpr int SZ = NDIM > 2 ? S : 1;
+    static constexpr int SP = S * SY * SZ;
+};
+
+// acc += v w_x w_y w_z: a marker's contributions to its run.
+template <typename T, int NDIM, int S>
+__device__ __forceinline__ void run_add(T (&acc)[RunShape<NDIM, S>::SP], const T (&w)[3][S], T v) {
+    constexpr int SY = RunShape<NDIM, S>::SY, SZ = RunShape<NDIM, S>::SZ;
+    T wz[SZ];
+#pragma unroll
+    for (int z = 0; z < SZ; ++z) wz[z] = (NDIM > 2 ? w[2][z] : T(1)) * v;
+#pragma unroll
+    for (int x = 0; x < S; ++x)
+#pragma unroll
+        for (int y = 0; y < SY; ++y) {
+            const T wxy = NDIM > 2 ? w[0][x] * w[1][y] : (NDIM > 1 ? w[0][x] * (w[1][y] * v) : w[0][x] * v);
+#pragma unroll
+            for (int z = 0; z < SZ; ++z) {
+                T& r = acc[(x * SY + y) * SZ + z];
+                r = NDIM > 2 ? fma(wxy, wz[z], r) : r + wxy;
+            }
+        }
+}
+
+// Adds the run anchored at box entry `at` to the box (node (x, y, z) at at + x sa + y sb +
+// z se, shared-memory atomics) and empties it.
+template <typename T, int NDIM, int S>
+__device__ __forceinline__ void run_flush(T* box, int at, int sa, int sb, int se, T (&acc)[RunShape<NDIM, S>::SP]) {
+    constexpr int SY = RunShape<NDIM, S>::SY, SZ = RunShape<NDIM, S>::SZ;
+#pragma unroll
+    for (int x = 0; x < S; ++x)
+#pragma unroll
+        for (int y = 0; y < SY; ++y)
+#pragma unroll
+            for (int z = 0; z < SZ; ++z) {
+                atomicAdd(box + at + x * sa + y * sb + z * se, acc[(x * SY + y) * SZ + z]);
+                acc[(x * SY + y) * SZ + z] = T(0);
+            }
+}
+
+// The closing runs of a warp (key -1: none), added to the box. Lanes of one anchor form
+// contiguous groups in a sorted store; where groups of four or more lanes occur (the dense
+// cells of a beam) each group is summed across the warp first (a segmented suffix sum into
+// its first lane). Every lane of the warp calls it.
+template <typename T, int NDIM, int S>
+__device__ __forceinline__ void run_close(T* box, int key, int sa, int sb, int se,
+                                          T (&acc)[RunShape<NDIM, S>::SP]) {
+    constexpr int SP = RunShape<NDIM, S>::SP;
+    constexpr unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int tag = key >= 0 ? key : -2 - lane;
+    const unsigned peers = __match_any_sync(FULL, tag);
+    const int head = __ffs(peers) - 1;
+    const int size = __popc(peers);
+    const int biggest = __reduce_max_sync(FULL, size);
+    const bool contiguous = peers == ((size == 32 ? FULL : ((1u << size) - 1u)) << head);
+    if (biggest >= 4 && __all_sync(FULL, contiguous)) {
+        const int last = head + size - 1;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+#pragma unroll
+            for (int q = 0; q < SP; ++q) {
+                const T other = __shfl_down_sync(FULL, acc[q], o);
+                if (lane + o <= last) acc[q] += other;
+            }
+        }
+        if (key >= 0 && lane == head) run_flush<T, NDIM, S>(box, key, sa, sb, se, acc);
+    } else if (key >= 0) {
+        run_flush<T, NDIM, S>(box, key, sa, sb, se, acc);
+    }
+}
+
 // 4- or 8-byte asynchronous copy global -> shared (cp.async, completion by group).
 template <int BYTES>
 __device__ __forceinline__ void cp_async(void* dst, const void* src) {
@@ -631,7 +710,6 @@ __global__ void __launch_bounds__(kMaxBlock, MINB) scatter_segments_kernel(const
     constexpr int ROWS = NDIM + 1;
     constexpr int CH = kMaxBlock * K;
     constexpr int ROW = kMaxBlock * PITCH;
-    constexpr unsigned FULL = 0xffffffffu;
     // UNI >= 0: every axis has that boundary code (a compile-time constant)
     auto code = [&](int d) { return UNI >= 0 ? UNI : a.g.code[d]; };
     __shared__ int s_lo[3], s_hi[3], s_lo2[3], s_hi2[3];
@@ -645,7 +723,6 @@ __global__ void __launch_bounds__(kMaxBlock, MINB) scatter_segments_kernel(const
 #pragma unroll
     for (int d = 0; d < NDIM; ++d) half[d] = a.g.num[d] / 2;
     const int t = threadIdx.x;
-    const int lane = t & 31;
     const int64_t nchunks = (a.n + CH - 1) / CH;
     int64_t c_first, c_last;
     chunk_range(nchunks, c_first, c_last);
@@ -750,18 +827,6 @@ __global__ void __launch_bounds__(kMaxBlock, MINB) scatter_segments_kernel(const
 #pragma unroll
             for (int q = 0; q < SP; ++q) acc[q] = T(0);
             int key = -1;  // the anchor of the open run, -1: none
-            // adds the open run to the box and empties it
-            auto flush = [&](int at) {
-#pragma unroll
-                for (int x = 0; x < S; ++x)
-#pragma unroll
-                    for (int y = 0; y < SY; ++y)
-#pragma unroll
-                        for (int z = 0; z < SZ; ++z) {
-                            atomicAdd(tile + at + x * sa + y * sb + z * se, acc[(x * SY + y) * SZ + z]);
-                            acc[(x * SY + y) * SZ + z] = T(0);
-                        }
-            };
 #pragma unroll 1
             for (int s = 0; s < nmine; ++s) {
                 const T v = mine[NDIM * ROW + s];
@@ -779,45 +844,11 @@ __global__ void __launch_bounds__(kMaxBlock, MINB) scatter_segments_kernel(const
                         for (int z = 0; z < S; ++z) w[d][z] = T(z == 0);
                     }
                 }
-                if (k != key && key >= 0) flush(key);
-                T wz[SZ];
-#pragma unroll
-                for (int z = 0; z < SZ; ++z) wz[z] = (NDIM > 2 ? w[2][z] : T(1)) * v;
-#pragma unroll
-                for (int x = 0; x < S; ++x)
-#pragma unroll
-                    for (int y = 0; y < SY; ++y) {
-                        const T wxy = NDIM > 2 ? w[0][x] * w[1][y] : (NDIM > 1 ? w[0][x] * (w[1][y] * v) : w[0][x] * v);
-#pragma unroll
-                        for (int z = 0; z < SZ; ++z) {
-                            T& r = acc[(x * SY + y) * SZ + z];
-                            r = NDIM > 2 ? fma(wxy, wz[z], r) : r + wxy;
-                        }
-                    }
+                if (k != key && key >= 0) run_flush<T, NDIM, S>(tile, key, sa, sb, se, acc);
+                run_add<T, NDIM, S>(acc, w, v);
                 key = k;
             }
-            // the closing runs: lanes of one anchor form contiguous groups in a sorted store;
-            // such groups are summed across the warp (a segmented suffix sum) before the adds
-            const int tag = key >= 0 ? key : -2 - lane;
-            const unsigned peers = __match_any_sync(FULL, tag);
-            const int head = __ffs(peers) - 1;
-            const int size = __popc(peers);
-            const int biggest = __reduce_max_sync(FULL, size);
-            const bool contiguous = peers == ((size == 32 ? FULL : ((1u << size) - 1u)) << head);
-            if (biggest >= 4 && __all_sync(FULL, contiguous)) {
-                const int last = head + size - 1;
-#pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-#pragma unroll
-                    for (int q = 0; q < SP; ++q) {
-                        const T other = __shfl_down_sync(FULL, acc[q], o);
-                        if (lane + o <= last) acc[q] += other;
-                    }
-                }
-                if (key >= 0 && lane == head) flush(key);
-            } else if (key >= 0) {
-                flush(key);
-            }
+            run_close<T, NDIM, S>(tile, key, sa, sb, se, acc);
         } else {
             // no box: each live marker adds to global memory
 #pragma unroll 1
@@ -1023,13 +1054,11 @@ __global__ void __launch_bounds__(BLOCK, MINB) scatter_tiles_kernel(const NodeAr
     constexpr int ROWS = NDIM + 1;
     constexpr int ROW = BLOCK * PITCH;
     constexpr int H = P / 2;  // a stencil's anchor is its first node + H
-    constexpr unsigned FULL = 0xffffffffu;
     __shared__ TileLoop s_loop;
     __shared__ TileStep s_step;
     T* buf = reinterpret_cast<T*>(mpf_dynamic_smem);  // [ROWS][ROW]
     T* box = buf + ROWS * ROW;
     const int t = threadIdx.x;
-    const int lane = t & 31;
     // the tile shape: compile-time constants where the launch fixes them (TX, TY, TZ > 0),
     // so that the box strides and every stencil offset in the box are immediates
     const int tl[3] = {TX > 0 ? TX : a.tile[0], TY > 0 ? TY : a.tile[1], TZ > 0 ? TZ : a.tile[2]};
@@ -1094,18 +1123,6 @@ __global__ void __launch_bounds__(BLOCK, MINB) scatter_tiles_kernel(const NodeAr
         cp_async_wait_all();
         __syncthreads();
         const int nmine = min(K, max(0, per + (t < rem ? 1 : 0) - sub * K));
-        // adds the open run to the box and empties it
-        auto flush = [&](int at) {
-#pragma unroll
-            for (int x = 0; x < S; ++x)
-#pragma unroll
-                for (int y = 0; y < SY; ++y)
-#pragma unroll
-                    for (int z = 0; z < SZ; ++z) {
-                        atomicAdd(box + at + x * sa + y * sb + z * se, acc[(x * SY + y) * SZ + z]);
-                        acc[(x * SY + y) * SZ + z] = T(0);
-                    }
-        };
         // a run that ends: the plane of its window at the first node along the last axis is
         // complete whatever comes next, and every ending run adds it in the same
         // instructions. A run followed by the next cell along the last axis (anchor + 1, the
@@ -1174,44 +1191,11 @@ __global__ void __launch_bounds__(BLOCK, MINB) scatter_tiles_kernel(const NodeAr
                 continue;
             }
             if (k != key && key >= 0) end_run(key, P > 0 ? k - key : 0);
-            T wz[SZ];
-#pragma unroll
-            for (int z = 0; z < SZ; ++z) wz[z] = (NDIM > 2 ? w[2][z] : T(1)) * v;
-#pragma unroll
-            for (int x = 0; x < S; ++x)
-#pragma unroll
-                for (int y = 0; y < SY; ++y) {
-                    const T wxy = NDIM > 2 ? w[0][x] * w[1][y] : (NDIM > 1 ? w[0][x] * (w[1][y] * v) : w[0][x] * v);
-#pragma unroll
-                    for (int z = 0; z < SZ; ++z) {
-                        T& r = acc[(x * SY + y) * SZ + z];
-                        r = NDIM > 2 ? fma(wxy, wz[z], r) : r + wxy;
-                    }
-                }
+            run_add<T, NDIM, S>(acc, w, v);
             key = k;
         }
         if (!closing) continue;  // the runs go on in the piece's next sub-chunk
-        // the closing runs, as in the segment scatter
-        const int tag = key >= 0 ? key : -2 - lane;
-        const unsigned peers = __match_any_sync(FULL, tag);
-        const int head = __ffs(peers) - 1;
-        const int size = __popc(peers);
-        const int biggest = __reduce_max_sync(FULL, size);
-        const bool contiguous = peers == ((size == 32 ? FULL : ((1u << size) - 1u)) << head);
-        if (biggest >= 4 && __all_sync(FULL, contiguous)) {
-            const int last = head + size - 1;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-#pragma unroll
-                for (int q = 0; q < SP; ++q) {
-                    const T other = __shfl_down_sync(FULL, acc[q], o);
-                    if (lane + o <= last) acc[q] += other;
-                }
-            }
-            if (key >= 0 && lane == head) flush(key);
-        } else if (key >= 0) {
-            flush(key);
-        }
+        run_close<T, NDIM, S>(box, key, sa, sb, se, acc);
         // every run is closed (the other lanes of a group summed into its head)
 #pragma unroll
         for (int q = 0; q < SP; ++q) acc[q] = T(0);
@@ -1235,8 +1219,6 @@ template <typename T, int NDIM, int KIND, int P, int NC, int MINB, int TX = 0, i
 __global__ void __launch_bounds__(kMaxBlock, MINB) gather_tiles_kernel(const NodeArgs<T> a) {
     constexpr int S = P + 1;
     constexpr int H = P / 2;
-    constexpr int SY = NDIM > 1 ? S : 1;
-    constexpr int SZ = NDIM > 2 ? S : 1;
     __shared__ TileLoop s_loop;
     __shared__ TileStep s_step;
     T* box = reinterpret_cast<T*>(mpf_dynamic_smem);
@@ -1244,7 +1226,7 @@ __global__ void __launch_bounds__(kMaxBlock, MINB) gather_tiles_kernel(const Nod
     const int tl[3] = {TX > 0 ? TX : a.tile[0], TY > 0 ? TY : a.tile[1], TZ > 0 ? TZ : a.tile[2]};
     int ex[3] = {1, 1, 1};
     tile_box_extents<NDIM, P>(tl, ex);
-    // box strides in nodes: node (x, y, z) of anchor key is node key + x sa + y sb + z se
+    // box strides in nodes
     const int se = NDIM > 2 ? 1 : 0;
     const int sb = NDIM > 2 ? ex[2] : (NDIM > 1 ? 1 : 0);
     const int sa = NDIM > 2 ? ex[1] * ex[2] : (NDIM > 1 ? ex[1] : 1);
@@ -1320,53 +1302,28 @@ __global__ void __launch_bounds__(kMaxBlock, MINB) gather_tiles_kernel(const Nod
             }
             T w[3][S];
             int base[3] = {0, 0, 0};
-            int k = 0;
+            int boff[3] = {0, 0, 0};  // the stencil's first node in the box, per axis
             bool inside = true;
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
                 if (d < NDIM) {
                     const T rel = rel_from(x[d], a.g, d);
                     base[d] = axis_stencil<T, KIND, P>(rel, a.g.num[d], PERIODIC, w[d]);
-                    const int off = wrap_index(base[d] + H - blo[d], a.g.num[d]);
-                    inside = inside && (unsigned)off < (unsigned)tl[d];
-                    k += off * st[d];
+                    boff[d] = wrap_index(base[d] + H - blo[d], a.g.num[d]);
+                    inside = inside && (unsigned)boff[d] < (unsigned)tl[d];
                 } else {
 #pragma unroll
                     for (int z = 0; z < S; ++z) w[d][z] = T(z == 0);
                 }
             }
             T acc[NC];
+            if (inside) {  // the box: node (x, y, z) of the stencil at box node offb[0][x] + offb[1][y] + offb[2][z]
+                int offb[3][S];
 #pragma unroll
-            for (int c = 0; c < NC; ++c) acc[c] = T(0);
-            if (inside) {
+                for (int d = 0; d < 3; ++d)
 #pragma unroll
-                for (int x = 0; x < S; ++x) {
-                    T sx_[NC];
-#pragma unroll
-                    for (int c = 0; c < NC; ++c) sx_[c] = T(0);
-#pragma unroll
-                    for (int y = 0; y < SY; ++y) {
-                        T sy_[NC];
-#pragma unroll
-                        for (int c = 0; c < NC; ++c) sy_[c] = T(0);
-#pragma unroll
-                        for (int z = 0; z < SZ; ++z) {
-                            const T* p = box + (k + x * sa + y * sb + z * se) * NC;
-#pragma unroll
-                            for (int c = 0; c < NC; ++c) {
-                                if constexpr (NDIM > 2) sy_[c] = fma(w[2][z], p[c], sy_[c]);
-                                else sy_[c] += p[c];
-                            }
-                        }
-#pragma unroll
-                        for (int c = 0; c < NC; ++c) {
-                            if constexpr (NDIM > 1) sx_[c] = fma(w[1][y], sy_[c], sx_[c]);
-                            else sx_[c] += sy_[c];
-                        }
-                    }
-#pragma unroll
-                    for (int c = 0; c < NC; ++c) acc[c] = fma(w[0][x], sx_[c], acc[c]);
-                }
+                    for (int s = 0; s < S; ++s) offb[d][s] = d < NDIM ? (boff[d] + s) * st[d] : 0;
+                stencil_sum<T, NDIM, S, NC, false, int>(box, offb, w, NC, 0, acc);
             } else {  // not this tile's marker: the field in global memory
                 int off[3][S];
 #pragma unroll
