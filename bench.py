@@ -66,11 +66,13 @@ def parse() -> argparse.Namespace:
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-ref-cuda", action="store_true")
     p.add_argument("--no-extras", action="store_true", help="skip the other configurations' measurements")
-    p.add_argument("--serve-requests", type=int, default=1000, help="requests of the serving stream (0: skip)")
+    p.add_argument("--serve-requests", type=int, default=10000, help="requests of the serving stream (0: skip)")
     p.add_argument("--paths-only", type=int, default=0, metavar="N",
                    help="measure only the path deposits, at N paths on 128^3 (a profiling case)")
     p.add_argument("--serve-rate", type=float, default=20000.0,
                    help="Poisson arrival rate of the stream, per s (the default outruns both arms: capacity)")
+    p.add_argument("--serve-latency-rate", type=float, default=1500.0,
+                   help="a second, sustainable arrival rate at which latencies are reported (0: skip)")
     return p.parse_args()
 
 
@@ -482,7 +484,15 @@ def run_ours(args, world, rank, local) -> None:
             extras["serving"]["what"] = (
                 "mixed stream (Poisson arrivals, ndim 1-3, nodes per axis log-U[32,256], markers log-U[1e3,1e7], "
                 "degree 1-3, gather 3-comp / scatter / path deposit, FP64, 120 GB budget) served with continuous "
-                "batching vs one plain launch per request; latency = completion - arrival")
+                "batching vs one plain launch per request; latency = completion - arrival; at this rate both arms "
+                "are saturated (requests/s = capacity, latency mostly queueing)")
+            if args.serve_latency_rate > 0:
+                torch.cuda.empty_cache()
+                at_rate = serving.serve_benchmark(args.serve_requests, args.serve_latency_rate, seed=0, device=device)
+                extras["serving"]["at_sustainable_rate"] = {
+                    "rate_per_s": args.serve_latency_rate, "served": at_rate["served"],
+                    "one_launch_per_request": at_rate["one_launch_per_request"],
+                    "what": "the same stream arriving at a rate below both arms' capacity: latencies"}
 
     clock = clocks.summary()
     if rank == 0:
@@ -639,25 +649,31 @@ def measure_autograd(device, reps: int) -> dict:
 
 
 def measure_deterministic(step, ps, ws, reps: int) -> dict:
-    """The bit-reproducible scatter on the headline store: time, identical bits on a repeat,
-    and its largest difference from the FP64 atomic scatter (relative to max |density|)."""
+    """The bit-reproducible scatter on the headline store (its tile form, with the store's
+    tile starts; the plain form beside it): time, identical bits on a repeat and between
+    the two forms, and the largest difference from the FP64 atomic scatter (relative to
+    max |density|)."""
     from mpifield_b200 import _lib
     from mpifield_b200.kernels import scatter_deterministic
 
     density = torch.zeros_like(step.density)
     workspace = torch.empty(16 * density.numel() + 4096, dtype=torch.uint8, device=ps.device)
 
-    def go():
+    def go(order):
         density.zero_()
-        scatter_deterministic(_lib.QUADRATIC, 2, ps, ws, density, step.geom, workspace)
+        scatter_deterministic(_lib.QUADRATIC, 2, ps, ws, density, step.geom, workspace, order=order)
 
-    ms = _event_ms(go, reps)
+    plain_ms = _event_ms(lambda: go(None), reps)
+    plain = density.clone()
+    ms = _event_ms(lambda: go(step.order), reps)
     first = density.clone()
-    go()
+    go(step.order)
     same = bool(torch.equal(first.view(torch.int64), density.view(torch.int64)))
+    same_forms = bool(torch.equal(first.view(torch.int64), plain.view(torch.int64)))
     step.gather_scatter(ps, ws)
     diff = float((density - step.density).abs().max() / step.density.abs().max())
     return {"value": ps.shape[1] / (ms / 1000.0), "unit": "markers/s", "ms": ms, "bitwise_repeatable": same,
+            "plain_form_ms": plain_ms, "same_bits_as_plain_form": same_forms,
             "max_rel_diff_vs_atomic_scatter": diff}
 
 

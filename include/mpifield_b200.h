@@ -107,6 +107,20 @@ MPF_API int mpf_gather(int kind, int degree, int ndim, const void* positions, in
                int dtype, const mpf_tuning* tuning, void* stream);
 
 /*
+ * mpf_scatter_deterministic for markers sorted by cell tile (tile and tile_start as for
+ * mpf_scatter_tiles): the same bits as mpf_scatter_deterministic on the same arguments,
+ * whatever the order of the markers. With one component and every axis periodic, each
+ * tile's fixed-point sums are gathered in shared memory and added to the workspace once per
+ * tile; otherwise mpf_scatter_deterministic's kernel runs. No counterpart in the reference.
+ */
+MPF_API int mpf_scatter_deterministic_tiles(int kind, int degree, int ndim, const void* positions,
+                                            int64_t pos_stride, const void* values, int64_t val_stride,
+                                            int64_t n, void* field, int64_t ncomp, const double* lower,
+                                            const double* cell, const int32_t* num, const int32_t* code,
+                                            const int32_t* tile, const int64_t* tile_start, void* workspace,
+                                            size_t workspace_bytes, void* stream);
+
+/*
  * mpf_gather for markers sorted by cell tile: positions in the rank order of
  * mpf_sort_by_tile (keys of the same kind, degree, geometry and `tile`), tile_start its
  * num_tiles + 2 starts (8-byte aligned device memory). The result is mpf_gather's, bit for

@@ -89,6 +89,8 @@ _SIGNATURES = {
     "mpf_unpermute_rows": ([_P, _L, _P, _L, _L, _P, _L, _I, _P], _I),
     "mpf_scatter_deterministic_workspace_bytes": ([_L, _P], _I),
     "mpf_scatter_deterministic": ([_I, _I, _I, _P, _L, _P, _L, _L, _P, _L, _P, _P, _P, _P, _P, C.c_size_t, _P], _I),
+    "mpf_scatter_deterministic_tiles": ([_I, _I, _I, _P, _L, _P, _L, _L, _P, _L, _P, _P, _P, _P, _P, _P, _P,
+                                         C.c_size_t, _P], _I),
     "mpf_batch_request_size": ([], _L),
     "mpf_batch_request_init": ([_P, _I, _I, _I, _I, _P, _L, _P, _L, _L, _P, _P, _L, _I, _P, _P, _P, _P], _I),
     "mpf_batch_launch": ([_P, _P, _I, _I, _P], _I),

@@ -321,15 +321,23 @@ int mpf_scatter_deterministic_workspace_bytes(int64_t entries, size_t* bytes) {
     return MPF_OK;
 }
 
-int mpf_scatter_deterministic(int kind, int degree, int ndim, const void* positions, int64_t pos_stride,
-                              const void* values, int64_t val_stride, int64_t n, void* field, int64_t ncomp,
-                              const double* lower, const double* cell, const int32_t* num, const int32_t* code,
-                              void* workspace, size_t workspace_bytes, void* stream) {
+// mpf_scatter_deterministic and its tile-sorted form (tile null: markers in any order).
+static int scatter_deterministic(int kind, int degree, int ndim, const void* positions, int64_t pos_stride,
+                                 const void* values, int64_t val_stride, int64_t n, void* field, int64_t ncomp,
+                                 const double* lower, const double* cell, const int32_t* num, const int32_t* code,
+                                 const int32_t* tile, const int64_t* tile_start, void* workspace,
+                                 size_t workspace_bytes, void* stream) {
     if (!valid_kind(kind, degree)) return MPF_ERR_ARGUMENT;
     MPF_TRY(check_grid(kind, degree, ndim, lower, cell, num, code));
     if (n < 0 || ncomp < 1 || ncomp > (1 << 20)) return MPF_ERR_ARGUMENT;
     MPF_TRY(check_rows(positions, pos_stride, n, ndim, MPF_F64));
     MPF_TRY(check_rows(values, val_stride, n, (int)ncomp, MPF_F64));
+    int64_t ntiles = 0;
+    if (tile) {
+        MPF_TRY(mpf_num_tiles(kind, degree, ndim, num, code, tile, &ntiles));
+        if (!tile_start) return MPF_ERR_ARGUMENT;
+        if (reinterpret_cast<uintptr_t>(tile_start) % alignof(int64_t) != 0) return MPF_ERR_ALIGNMENT;
+    }
     if (n == 0) return MPF_OK;
     if (!field) return MPF_ERR_ARGUMENT;
     if (!aligned(field, MPF_F64)) return MPF_ERR_ALIGNMENT;
@@ -343,7 +351,26 @@ int mpf_scatter_deterministic(int kind, int degree, int ndim, const void* positi
     a.pos = (const double*)positions; a.pos_stride = pos_stride;
     a.values = (const double*)values; a.val_stride = val_stride;
     a.field_out = (double*)field; a.n = n; a.ncomp = (int)ncomp;
+    if (tile) set_tiles(a, ndim, degree, num, code, tile, tile_start, ntiles);
     return launch_scatter_deterministic(kind, degree, ndim, a, entries, workspace, static_cast<cudaStream_t>(stream));
+}
+
+int mpf_scatter_deterministic(int kind, int degree, int ndim, const void* positions, int64_t pos_stride,
+                              const void* values, int64_t val_stride, int64_t n, void* field, int64_t ncomp,
+                              const double* lower, const double* cell, const int32_t* num, const int32_t* code,
+                              void* workspace, size_t workspace_bytes, void* stream) {
+    return scatter_deterministic(kind, degree, ndim, positions, pos_stride, values, val_stride, n, field, ncomp,
+                                 lower, cell, num, code, nullptr, nullptr, workspace, workspace_bytes, stream);
+}
+
+int mpf_scatter_deterministic_tiles(int kind, int degree, int ndim, const void* positions, int64_t pos_stride,
+                                    const void* values, int64_t val_stride, int64_t n, void* field, int64_t ncomp,
+                                    const double* lower, const double* cell, const int32_t* num,
+                                    const int32_t* code, const int32_t* tile, const int64_t* tile_start,
+                                    void* workspace, size_t workspace_bytes, void* stream) {
+    if (!tile) return MPF_ERR_ARGUMENT;
+    return scatter_deterministic(kind, degree, ndim, positions, pos_stride, values, val_stride, n, field, ncomp,
+                                 lower, cell, num, code, tile, tile_start, workspace, workspace_bytes, stream);
 }
 
 int mpf_gather_grad(int kind, int degree, int ndim, const void* positions, int64_t pos_stride, int64_t n,

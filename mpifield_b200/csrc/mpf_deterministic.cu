@@ -13,7 +13,7 @@
 // The values must be finite (a non-finite value has no fixed-point image).
 #include <cmath>
 
-#include "mpf_nodes.cuh"
+#include "mpf_nodes_launch.cuh"
 #include "mpifield_b200.h"
 
 namespace mpf {
@@ -108,6 +108,160 @@ __global__ void __launch_bounds__(256) det_scatter_kernel(const NodeArgs<double>
     }
 }
 
+// The bit-reproducible scatter for markers sorted by cell tile (mpf_sort_by_tile), one
+// component, every axis periodic: the same fixed-point contributions as det_scatter_kernel,
+// summed per tile in a shared-memory box of integer pairs (shared-memory integer atomics)
+// and added to the node accumulators once per tile piece, instead of two global atomics per
+// contribution. Integer sums are exact, so the accumulators -- and the field -- have the
+// same bits as with det_scatter_kernel. The CTA's share of the ranks is cut at tile
+// boundaries as in the tile scatter; markers go to threads in stride; a marker whose anchor
+// is not in its rank's tile adds to the node accumulators directly.
+template <int NDIM, int KIND, int P, int TX = 0, int TY = 0, int TZ = 0>
+__global__ void __launch_bounds__(kMaxBlock, 3) det_scatter_tiles_kernel(const NodeArgs<double> a, long long* hi,
+                                                                        long long* lo, const DetHeader* h) {
+    constexpr int S = P + 1;
+    constexpr int H = P / 2;
+    constexpr int SY = NDIM > 1 ? S : 1;
+    constexpr int SZ = NDIM > 2 ? S : 1;
+    __shared__ TileLoop s_loop;
+    __shared__ TileStep s_step;
+    const int t = threadIdx.x;
+    const int tl[3] = {TX > 0 ? TX : a.tile[0], TY > 0 ? TY : a.tile[1], TZ > 0 ? TZ : a.tile[2]};
+    int ex[3] = {1, 1, 1};
+    tile_box_extents<NDIM, P>(tl, ex);
+    const int total = ex[0] * ex[1] * ex[2];
+    unsigned long long* bhi = reinterpret_cast<unsigned long long*>(mpf_dynamic_smem);
+    unsigned long long* blo = bhi + total;
+    for (int q = t; q < 2 * total; q += kMaxBlock) bhi[q] = 0ull;
+    const int se = NDIM > 2 ? 1 : 0;
+    const int sb = NDIM > 2 ? ex[2] : (NDIM > 1 ? 1 : 0);
+    const int sa = NDIM > 2 ? ex[1] * ex[2] : (NDIM > 1 ? ex[1] : 1);
+    const int st[3] = {sa, NDIM > 1 ? sb : 0, NDIM > 2 ? se : 0};
+    if (t == 0) {
+        const int64_t live = min(max(__ldg(a.tile_start + a.ntiles), (int64_t)0), a.n);
+        const int64_t per = (live + gridDim.x - 1) / gridDim.x;
+        s_loop.m = min((int64_t)blockIdx.x * per, live);
+        s_loop.m_end = min(s_loop.m + per, live);
+        s_loop.e = s_loop.m;
+        s_loop.cur = -1;
+        s_loop.sub = s_loop.nsub = 0;
+        s_loop.part = s_loop.extra = 0;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) s_step.blo[d] = s_step.old_lo[d] = 0;
+    }
+    const int f = det_scale(h, a.n);
+    const double low = ldexp(1.0, kLowBits);
+#pragma unroll 1
+    for (;;) {
+        if (t == 0) plan_tile_step<NDIM, H>(s_loop, s_step, a.tile_start, a.ntiles, a.tiles, tl, 1 << 28);
+        // the plan is visible and the previous piece's adds are complete
+        __syncthreads();
+        const int64_t first = s_step.first;
+        const int count = s_step.count;
+        if (s_step.retire) {
+            const int olo[3] = {s_step.old_lo[0], s_step.old_lo[1], s_step.old_lo[2]};
+            for_box_entries<NDIM>(olo, ex, a.g.num, a.g.ext, [&](int e, auto node) {
+                const unsigned long long vh = bhi[e], vl = blo[e];
+                if (vh != 0ull || vl != 0ull) {
+                    const int64_t at = node();
+                    atomicAdd(reinterpret_cast<unsigned long long*>(hi + at), vh);
+                    atomicAdd(reinterpret_cast<unsigned long long*>(lo + at), vl);
+                    bhi[e] = 0ull;
+                    blo[e] = 0ull;
+                }
+            });
+            __syncthreads();
+        }
+        if (count == 0) break;
+        const int blo_[3] = {s_step.blo[0], s_step.blo[1], s_step.blo[2]};
+        // thread t takes the t-th of kMaxBlock contiguous ranges of the piece, so that the
+        // lanes of a warp add to different cells at a time (same-address integer atomics of
+        // one instruction serialise)
+        const int per = count / kMaxBlock, rem = count % kMaxBlock;
+        const int j0 = t * per + min(t, rem), j1 = j0 + per + (t < rem ? 1 : 0);
+#pragma unroll 1
+        for (int j = j0; j < j1; ++j) {
+            const int64_t i = first + j;
+            const double v = a.values[i];
+            if (v == 0.0) continue;  // a dead marker deposits nothing and its position is not read
+            double w[3][S];
+            int base[3] = {0, 0, 0};
+            int k = 0;
+            bool inside = true;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                if (d < NDIM) {
+                    base[d] = axis_stencil<double, KIND, P>(rel_of(a, d, i), a.g.num[d], PERIODIC, w[d]);
+                    const int off = wrap_index(base[d] + H - blo_[d], a.g.num[d]);
+                    inside = inside && (unsigned)off < (unsigned)tl[d];
+                    k += off * st[d];
+                } else {
+#pragma unroll
+                    for (int s = 0; s < S; ++s) w[d][s] = double(s == 0);
+                }
+            }
+            int64_t goff[3][S];
+            if (!inside) global_offsets<NDIM, S>(base, a.g.num, a.g.code, a.g.ext, goff);
+#pragma unroll
+            for (int x = 0; x < S; ++x)
+#pragma unroll
+                for (int y = 0; y < SY; ++y)
+#pragma unroll
+                    for (int z = 0; z < SZ; ++z) {
+                        double wt = w[0][x];
+                        if (NDIM > 1) wt *= w[1][y];
+                        if (NDIM > 2) wt *= w[2][z];
+                        const double scaled = ldexp(wt * v, f);  // exact scaling by a power of two
+                        const double whole = rint(scaled);
+                        const long long part = (long long)whole;
+                        const long long rest = (long long)rint((scaled - whole) * low);
+                        if (inside) {
+                            const int e = k + x * sa + y * sb + z * se;
+                            atomicAdd(bhi + e, (unsigned long long)part);
+                            atomicAdd(blo + e, (unsigned long long)rest);
+                        } else {
+                            const int64_t at = goff[0][x] + goff[1][y] + goff[2][z];
+                            atomicAdd(reinterpret_cast<unsigned long long*>(hi + at), (unsigned long long)part);
+                            atomicAdd(reinterpret_cast<unsigned long long*>(lo + at), (unsigned long long)rest);
+                        }
+                    }
+        }
+    }
+}
+
+// The tile form when it applies (tile starts given, one component, periodic axes, the box
+// of integer pairs within a third of an SM's shared memory); MPF_ERR_ARGUMENT otherwise.
+template <int NDIM, int KIND, int P>
+static int det_tiles_launch(const NodeArgs<double>& a, long long* hi, long long* lo, const DetHeader* h,
+                            cudaStream_t s) {
+    if (!a.tile_start || a.ncomp != 1 || !all_periodic<double, NDIM>(a)) return MPF_ERR_ARGUMENT;
+    int64_t total = 1;
+    for (int d = 0; d < NDIM; ++d) {
+        int64_t e = (int64_t)a.tile[d] + P;
+        if (d == NDIM - 1 && (e & 1) == 0) ++e;
+        total *= e;
+    }
+    const int64_t box_bytes = 2 * total * (int64_t)sizeof(long long);
+    if (box_bytes > (228 * 1024) / 3 - 2048) return MPF_ERR_ARGUMENT;
+    const int smem = (int)box_bytes;
+    auto kernel = det_scatter_tiles_kernel<NDIM, KIND, P>;
+    int shape = 0;
+    if constexpr (NDIM == 3 && P == 2) {
+        if (a.tile[0] == 4 && a.tile[1] == 4 && a.tile[2] == 64) {
+            kernel = det_scatter_tiles_kernel<NDIM, KIND, P, 4, 4, 64>;
+            shape = 1;
+        } else if (a.tile[0] == 8 && a.tile[1] == 8 && a.tile[2] == 8) {
+            kernel = det_scatter_tiles_kernel<NDIM, KIND, P, 8, 8, 8>;
+            shape = 2;
+        }
+    }
+    static int cache[3][64] = {{0}};
+    if (allow_smem(kernel, smem, cache[shape]) != MPF_OK) return MPF_ERR_CUDA;
+    const int64_t units = (a.n + kMaxBlock - 1) / kMaxBlock;
+    kernel<<<grid_for(units, smem, kMaxBlock, 3), kMaxBlock, smem, s>>>(a, hi, lo, h);
+    return MPF_OK;
+}
+
 __global__ void det_finish_kernel(double* field, const long long* hi, const long long* lo, int64_t entries,
                                   const DetHeader* h, int64_t n) {
     const int f = det_scale(h, n);
@@ -122,6 +276,7 @@ size_t det_workspace_bytes(int64_t entries) { return sizeof(DetHeader) + 2 * (si
 template <int NDIM, int KIND, int P>
 static void det_launch(const NodeArgs<double>& a, long long* hi, long long* lo, int64_t entries, const DetHeader* h,
                        cudaStream_t s) {
+    if (det_tiles_launch<NDIM, KIND, P>(a, hi, lo, h, s) != MPF_ERR_ARGUMENT) return;  // launched, or a CUDA error
     const int64_t blocks = std::min<int64_t>((a.n + 255) / 256, (int64_t)sm_count() * 8);
     det_scatter_kernel<NDIM, KIND, P><<<(unsigned)std::max<int64_t>(blocks, 1), 256, 0, s>>>(a, hi, lo, entries, h);
 }

@@ -908,13 +908,14 @@ __device__ __forceinline__ void tile_box_extents(const int* tile, int* ex) {
     if ((ex[NDIM - 1] & 1) == 0) ++ex[NDIM - 1];
 }
 
-// field += the non-zero entries of a tile's box (global atomics), and the box zeroed.
-// The box is row-major with extents ex; its entry (0, 0, 0) is the pre-mapping node lo
-// of a grid whose axes are all periodic. Thread t takes entries t, t + B, t + 2B, ...
-// (B = blockDim.x), its box coordinates found once and then advanced by those of B with
-// one carry per axis: no division per entry.
-template <typename T, int NDIM>
-__device__ __forceinline__ void flush_clear_box(T* box, T* field, const int* lo, const int* ex, const Grid<T>& g) {
+// Calls fn(e, at) for the entries e of a tile's box that this thread takes, at being the
+// entry's node index in the grid. The box is row-major with extents ex; its entry
+// (0, 0, 0) is the pre-mapping node lo of a grid whose axes are all periodic (num, ext).
+// Thread t takes entries t, t + B, t + 2B, ... (B = blockDim.x), its box coordinates found
+// once and then advanced by those of B with one carry per axis: no division per entry.
+template <int NDIM, typename F>
+__device__ __forceinline__ void for_box_entries(const int* lo, const int* ex, const int* num, const int* ext,
+                                                F&& fn) {
     int total = 1;
 #pragma unroll
     for (int d = 0; d < NDIM; ++d) total *= ex[d];
@@ -931,14 +932,12 @@ __device__ __forceinline__ void flush_clear_box(T* box, T* field, const int* lo,
     dc[0] = b;
 #pragma unroll 1
     for (int e = threadIdx.x; e < total; e += blockDim.x) {
-        const T v = box[e];
-        if (v != T(0)) {
-            box[e] = T(0);
+        fn(e, [&]() {
             int64_t at = 0;
 #pragma unroll
-            for (int d = 0; d < NDIM; ++d) at = at * g.ext[d] + wrap_index(lo[d] + c[d], g.num[d]);
-            atomicAdd(field + at, v);
-        }
+            for (int d = 0; d < NDIM; ++d) at = at * ext[d] + wrap_index(lo[d] + c[d], num[d]);
+            return at;
+        });
         int carry = 0;
 #pragma unroll
         for (int d = NDIM - 1; d >= 0; --d) {
@@ -950,6 +949,18 @@ __device__ __forceinline__ void flush_clear_box(T* box, T* field, const int* lo,
             }
         }
     }
+}
+
+// field += the non-zero entries of a tile's box (global atomics), and the box zeroed.
+template <typename T, int NDIM>
+__device__ __forceinline__ void flush_clear_box(T* box, T* field, const int* lo, const int* ex, const Grid<T>& g) {
+    for_box_entries<NDIM>(lo, ex, g.num, g.ext, [&](int e, auto node) {
+        const T v = box[e];
+        if (v != T(0)) {
+            box[e] = T(0);
+            atomicAdd(field + node(), v);
+        }
+    });
 }
 
 // The tile scatter: the segment scatter (above) for markers sorted by cell tile

@@ -189,9 +189,13 @@ def scatter(kind: int, degree: int, positions: torch.Tensor, values: torch.Tenso
 
 
 def scatter_deterministic(kind: int, degree: int, positions: torch.Tensor, values: torch.Tensor,
-                          field: torch.Tensor, geometry, workspace: torch.Tensor | None = None) -> None:
+                          field: torch.Tensor, geometry, workspace: torch.Tensor | None = None, order=None) -> None:
     """field(k, c) += sum_i W_k(x_i) values(c, i), the same bits for every run and marker
-    order (``mpf_scatter_deterministic``: fixed-point integer sums); float64 only."""
+    order (``mpf_scatter_deterministic``: fixed-point integer sums); float64 only.
+
+    ``order``: the `sorting.TileOrder` whose rank order the markers are in, for
+    ``mpf_scatter_deterministic_tiles`` (the same bits).
+    """
     lower, cell, num, code, ndim = _lib.geometry_arrays(geometry)
     device = _lib.require_cuda(positions, values, field)
     if field.dtype != torch.float64:
@@ -208,10 +212,16 @@ def scatter_deterministic(kind: int, degree: int, positions: torch.Tensor, value
     if workspace is None or workspace.numel() * workspace.element_size() < size.value:
         workspace = torch.empty(size.value, dtype=torch.uint8, device=device)
     out = _Output(shaped, torch.float64, accumulate=True)
-    status = _lib.library().mpf_scatter_deterministic(
-        kind, degree, ndim, pos.data_ptr(), ps, vals.data_ptr(), vs, pos.shape[1], out.work.data_ptr(), ncomp,
-        lower, cell, num, code, workspace.data_ptr(), workspace.numel() * workspace.element_size(),
-        _lib.stream_of(device))
+    wbytes = workspace.numel() * workspace.element_size()
+    if order is None:
+        status = _lib.library().mpf_scatter_deterministic(
+            kind, degree, ndim, pos.data_ptr(), ps, vals.data_ptr(), vs, pos.shape[1], out.work.data_ptr(), ncomp,
+            lower, cell, num, code, workspace.data_ptr(), wbytes, _lib.stream_of(device))
+    else:
+        tile, starts = _tile_args(order, ndim, device)
+        status = _lib.library().mpf_scatter_deterministic_tiles(
+            kind, degree, ndim, pos.data_ptr(), ps, vals.data_ptr(), vs, pos.shape[1], out.work.data_ptr(), ncomp,
+            lower, cell, num, code, tile, starts, workspace.data_ptr(), wbytes, _lib.stream_of(device))
     _lib.check(status, "scatter_deterministic")
     out.finish()
 
