@@ -495,6 +495,11 @@ class Server:
                         flying.remove(j)
                     result = j.buffers["out"].clone() if self.keep_results else None
                     done.append(Done(j.req, stamp - j.req.arrival, result))
+                if self.keep_results:
+                    # the copies run on this thread's stream: they are done before the memory
+                    # returns to the arena (a request admitted next writes it from another stream)
+                    torch.cuda.current_stream(self.device).synchronize()
+                for j in finished:
                     self.arena.release(j.block)
             elif not waiting and i < len(pending) and not flying and not in_batch and not batch_jobs:
                 # idle until the next arrival
