@@ -1172,10 +1172,22 @@ __global__ void __launch_bounds__(BLOCK, MINB) scatter_tiles_kernel(const NodeAr
                 for (int q = 0; q < SP; ++q) acc[q] = T(0);
             }
         };
+        // the next marker's position and value are read while the current one is worked on
+        T nx[4] = {T(0), T(0), T(0), T(0)};
+        if (nmine > 0) {
+#pragma unroll
+            for (int d = 0; d <= NDIM; ++d) nx[d] = buf[d * ROW + t * PITCH];
+        }
 #pragma unroll 1
         for (int s = 0; s < nmine; ++s) {
-            const int q = t * PITCH + s;
-            const T v = buf[NDIM * ROW + q];
+            T cx[4];
+#pragma unroll
+            for (int d = 0; d < 4; ++d) cx[d] = nx[d];
+            if (s + 1 < nmine) {
+#pragma unroll
+                for (int d = 0; d <= NDIM; ++d) nx[d] = buf[d * ROW + t * PITCH + s + 1];
+            }
+            const T v = cx[NDIM];
             if (v == T(0)) continue;
             T w[3][S];
             int base[3] = {0, 0, 0};
@@ -1184,7 +1196,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) scatter_tiles_kernel(const NodeAr
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
                 if (d < NDIM) {
-                    const T rel = rel_from(buf[d * ROW + q], a.g, d);
+                    const T rel = rel_from(cx[d], a.g, d);
                     base[d] = axis_stencil<T, KIND, P>(rel, a.g.num[d], PERIODIC, w[d]);
                     const int off = wrap_index(base[d] + H - blo[d], a.g.num[d]);
                     inside = inside && (unsigned)off < (unsigned)tl[d];
