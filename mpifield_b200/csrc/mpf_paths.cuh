@@ -710,9 +710,9 @@ __global__ void __launch_bounds__(256) deposit_paths_tiled_kernel(const PathArgs
     if (have_box) flush_edge_box<T, NDIM>(tile, a.edges_out, sink, a.g);
 }
 
-// One thread per path, global atomics.
-template <typename T, int NDIM, int P, bool WHITNEY>
-__global__ void __launch_bounds__(256, 1) deposit_paths_kernel(const PathArgs<T> a) {
+// One thread per path, global atomics; BLOCK threads, at least MINB CTAs per SM.
+template <typename T, int NDIM, int P, bool WHITNEY, int BLOCK = 256, int MINB = 1>
+__global__ void __launch_bounds__(BLOCK, MINB) deposit_paths_kernel(const PathArgs<T> a) {
     GlobalEdgeSink<T, NDIM> sink;
     sink.edges = a.edges_out;
 #pragma unroll

@@ -27,10 +27,12 @@ def cu(a, dtype=torch.float64):
     return torch.as_tensor(np.ascontiguousarray(a), dtype=dtype, device=DEV)
 
 
-# one thread per path with global atomics (the default), the tiled deposit (shared-memory
-# edge boxes, path 2) and the same with boxes too small for most chunks
+# one thread per path with global atomics (the default; variant 1 the launch of one CTA
+# per SM), the tiled deposit (shared-memory edge boxes, path 2) and the same with boxes
+# too small for most chunks
 TUNINGS = {"direct": None, "tiled": _lib.tuning_struct(_lib.PATH_STAGED),
-           "small_box": _lib.tuning_struct(_lib.PATH_STAGED, smem_bytes=2048, block=2)}
+           "small_box": _lib.tuning_struct(_lib.PATH_STAGED, smem_bytes=2048, block=2),
+           "direct_one_cta": _lib.tuning_struct(variant=1)}
 
 
 def run_deposit(kind, degree, start, end, charges, shape, geom, dtype=torch.float64, tuning="direct"):
