@@ -10,7 +10,7 @@ weights uniform in [0.5, 1.5]. All inputs are synthetic (there is no dataset).
 
 The marker store is kept in cell-tile order, as particle-in-cell codes keep their
 markers (picnic's sort_by_cell): the markers are sorted once before timing (tiles of
-8^3 cells, cells in a tile in row-major order: mpifield_b200.sort_by_tile(within=True)).
+4 x 4 x 64 cells, cells in a tile in row-major order: mpifield_b200.sort_by_tile(within=True)).
 One step = gather E (3, N) from the field at the markers + scatter the weights into a
 zeroed 1-component density. `value` is N / step time with every input resident in HBM.
 `full_step` times the whole path from markers in random order instead: tile sort,
@@ -567,19 +567,32 @@ def measure_fp32(step, ps, ws, reps: int) -> dict:
                     "to float32); error relative to max |float64 result|"}
 
 
-def measure_paths(device, reps: int, peak: float, n: int = 1 << 25) -> dict:
-    """The path deposit: 128^3 periodic, N = 2^25 paths, start uniform, end = start +
-    U[-0.9, 0.9] cells per axis, charges U[0.5, 1.5]; WHITNEY and QUADRATIC_EDGES, paths in
-    random order and sorted by the start's cell tile; continuity residual
-    max |rho(end) - rho(start) - G^T J| with the node deposit of the same degree."""
+PATH_GRID = 128
+
+
+def path_case(device, n: int = 1 << 25, seed: int = 7):
+    """The path-deposit workload: 128^3 periodic on the unit cube, start uniform, end =
+    start + U[-0.9, 0.9] cells per axis, charges U[0.5, 1.5] (dt = 1). Returns start,
+    end (3, n), charges (1, n) and the `BlockGrid`."""
     import mpifield_b200 as mf
 
-    g_n = 128
-    g = torch.Generator(device=device).manual_seed(7)
+    g_n = PATH_GRID
+    g = torch.Generator(device=device).manual_seed(seed)
     start = torch.rand((3, n), generator=g, device=device, dtype=torch.float64)
     end = start + (torch.rand((3, n), generator=g, device=device, dtype=torch.float64) * 1.8 - 0.9) / g_n
     q = torch.rand((1, n), generator=g, device=device, dtype=torch.float64) + 0.5
     grid = mf.BlockGrid.from_geometry((0.0,) * 3, (1.0 / g_n,) * 3, (g_n,) * 3, (True,) * 3)
+    return start, end, q, grid
+
+
+def measure_paths(device, reps: int, peak: float, n: int = 1 << 25) -> dict:
+    """The path deposit on `path_case`: WHITNEY and QUADRATIC_EDGES, paths in random order
+    and sorted by the start's cell tile; continuity residual max |rho(end) - rho(start) -
+    G^T J| with the node deposit of the same degree."""
+    import mpifield_b200 as mf
+
+    g_n = PATH_GRID
+    start, end, q, grid = path_case(device, n)
     geom = grid.geometry
     t = mf.sort_by_tile(start, mf.LINEAR, geom, TILE, within=True)
     s_start, s_end, s_q = mf.permute(start, t.order), mf.permute(end, t.order), mf.permute(q, t.order)
@@ -677,6 +690,21 @@ def measure_deterministic(step, ps, ws, reps: int) -> dict:
             "max_rel_diff_vs_atomic_scatter": diff}
 
 
+def plain_2d_case():
+    """The plain 2D workload: 101 x 51 nodes on [0, 0.1] x [0, 0.05], bounded (geometry);
+    N = 100,000 uniform markers from numpy default_rng(0) (2, N); E = -gradient(phi),
+    phi = 1000 exp(-((x - 0.05)^2 + (y - 0.025)^2) / 1e-4), by numpy.gradient (101, 51, 2)."""
+    nx, ny, n = 101, 51, 100_000
+    hx, hy = 0.1 / (nx - 1), 0.05 / (ny - 1)
+    geom = (0.0, 0.0, hx, hy, nx, ny, 0, 0)
+    X, Y = np.meshgrid(np.linspace(0, 0.1, nx), np.linspace(0, 0.05, ny), indexing="ij")
+    phi = 1000.0 * np.exp(-((X - 0.05) ** 2 + (Y - 0.025) ** 2) / 1e-4)
+    ex, ey = np.gradient(phi, hx, hy)
+    rng = np.random.default_rng(0)
+    pos = np.stack([rng.uniform(0, 0.1, n), rng.uniform(0, 0.05, n)])
+    return geom, pos, np.stack([-ex, -ey], axis=-1)
+
+
 def measure_plain_2d(device, reps: int) -> dict:
     """The plain 2D configuration: 101 x 51 nodes on [0, 0.1] x [0, 0.05], bounded; LINEAR;
     E = -gradient(phi), phi = 1000 exp(-((x - 0.05)^2 + (y - 0.025)^2) / 1e-4); N = 100,000
@@ -684,15 +712,10 @@ def measure_plain_2d(device, reps: int) -> dict:
     kernels on the block itself (its halo nodes trimmed at the bounded walls)."""
     import mpifield_b200 as mf
 
-    nx, ny, n = 101, 51, 100_000
-    hx, hy = 0.1 / (nx - 1), 0.05 / (ny - 1)
-    geom = (0.0, 0.0, hx, hy, nx, ny, 0, 0)
-    X, Y = np.meshgrid(np.linspace(0, 0.1, nx), np.linspace(0, 0.05, ny), indexing="ij")
-    phi = 1000.0 * np.exp(-((X - 0.05) ** 2 + (Y - 0.025) ** 2) / 1e-4)
-    ex, ey = np.gradient(phi, hx, hy)
-    E = torch.tensor(np.stack([-ex, -ey], axis=-1), device=device)
-    rng = np.random.default_rng(0)
-    pos = torch.tensor(np.stack([rng.uniform(0, 0.1, n), rng.uniform(0, 0.05, n)]), device=device)
+    geom, pos_np, E_np = plain_2d_case()
+    nx, ny, n = geom[4], geom[5], pos_np.shape[1]
+    E = torch.tensor(E_np, device=device)
+    pos = torch.tensor(pos_np, device=device)
     ones = torch.ones((1, n), dtype=torch.float64, device=device)
     rho = torch.zeros((nx, ny, 1), dtype=torch.float64, device=device)
     out_e = torch.empty((2, n), dtype=torch.float64, device=device)

@@ -72,6 +72,9 @@ typedef struct mpf_tuning {
     int32_t smem_bytes;  /* dynamic shared memory per CTA for a box; 0: default */
     int32_t ctas_per_sm; /* resident CTAs per SM the grid is sized for; 0: default */
     int32_t variant;     /* kernel variant; 0: the default for the shape (see mpf_gather, mpf_scatter) */
+    int32_t wait_limit;  /* tries of a bounded wait on a bulk copy before the CTA gives up and raises
+                            MPF_DEVICE_ERROR_WAIT; 0: the default (far beyond any copy of a working
+                            device), < 0: none (gives up at once: a test of the give-up path) */
 } mpf_tuning;
 
 /* The library version, e.g. 10000 for 1.0.0. */
@@ -279,16 +282,20 @@ MPF_API int mpf_sort_by_tile(int kind, int degree, int ndim, const void* positio
                      int dtype, void* stream);
 
 /*
- * mpf_sort_by_tile without a workspace argument and without any allocation, for callers
- * that cannot call cudaMalloc: work recorded into a CUDA graph (an allocation cannot be
- * captured), a host application that owns all device memory through its own pool, or a
- * real-time loop that cannot take the implicit synchronisation of an allocation. The
- * workspace is a fixed array inside the library (about 18 MB per GPU that loads it, held
- * until the process exits), so n is at most MPF_NOALLOC_MAX_MARKERS; larger n returns
- * MPF_ERR_WORKSPACE before any device work. The first call on a device looks the array up
- * (once per device, with that device current); make that first call before any stream
- * capture. All calls share the array: calls that overlap on the GPU race. No counterpart
- * in the reference.
+ * mpf_sort_by_tile without a workspace argument and without any allocation. No
+ * counterpart in the reference. It is for callers that cannot call cudaMalloc: a host
+ * application that gives all device memory to its own pool or arena at start-up and
+ * allows no allocation afterwards, or a real-time loop that cannot take the implicit
+ * device synchronisation an allocation may bring. The workspace is a fixed array inside
+ * the library (about 18 MB on every GPU that loads it, held until the process exits), so
+ * n is at most MPF_NOALLOC_MAX_MARKERS; a larger n returns MPF_ERR_WORKSPACE and a bad
+ * argument its status, both before any CUDA call. The array's device address is looked
+ * up with cudaGetSymbolAddress on the first call on a device (with that device current,
+ * again in a new context); that first call may also load the library's device code, so
+ * make it before any stream capture on that device. Safe to call from several host
+ * threads, but all calls share the array: calls that overlap on the GPU race, so order
+ * them on one stream or with events. The array keeps the last call's contents; no part
+ * of the sort needs a starting value in it.
  */
 #define MPF_NOALLOC_MAX_MARKERS (1 << 20)
 MPF_API int mpf_sort_by_tile_noalloc(int kind, int degree, int ndim, const void* positions,

@@ -34,10 +34,10 @@ class BackendError(RuntimeError):
 
 
 class Tuning(C.Structure):
-    """``mpf_tuning``: the path, CTA size, shared memory, CTAs per SM and kernel variant of a launch."""
+    """``mpf_tuning``: the path, CTA size, shared memory, CTAs per SM, kernel variant and wait limit of a launch."""
 
     _fields_ = [("path", C.c_int32), ("block", C.c_int32), ("smem_bytes", C.c_int32),
-                ("ctas_per_sm", C.c_int32), ("variant", C.c_int32)]
+                ("ctas_per_sm", C.c_int32), ("variant", C.c_int32), ("wait_limit", C.c_int32)]
 
 
 class BatchRequest(C.Structure):
@@ -181,8 +181,8 @@ def geometry_arrays(geometry) -> tuple[C.Array, C.Array, C.Array, C.Array, int]:
 
 
 def tuning_struct(path: int = PATH_AUTO, block: int = 0, smem_bytes: int = 0, ctas_per_sm: int = 0,
-                  variant: int = 0) -> Tuning:
-    return Tuning(path, block, smem_bytes, ctas_per_sm, variant)
+                  variant: int = 0, wait_limit: int = 0) -> Tuning:
+    return Tuning(path, block, smem_bytes, ctas_per_sm, variant, wait_limit)
 
 
 def device_errors(clear: bool = True) -> int:

@@ -3,6 +3,7 @@
 // weighting.py:91-97,156-164 and edges.py:145-167,210-213, become status codes here) and
 // the dispatch to the typed launchers.
 #include <atomic>
+#include <mutex>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -27,17 +28,54 @@ int record_cuda_error(cudaError_t e) {
 
 int launch_status() { return record_cuda_error(cudaGetLastError()); }
 
+// The driver's cuCtxGetCurrent and cuCtxGetId, reached through the runtime (the library
+// does not link the driver library itself); null where the driver lacks them.
+using CtxGetCurrentFn = int (*)(void** ctx);
+using CtxGetIdFn = int (*)(void* ctx, unsigned long long* id);
+static std::once_flag g_ctx_once;
+static CtxGetCurrentFn g_ctx_get_current = nullptr;
+static CtxGetIdFn g_ctx_get_id = nullptr;
+
+unsigned long long current_context_id() {
+    std::call_once(g_ctx_once, [] {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult found;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &found) == cudaSuccess &&
+            found == cudaDriverEntryPointSuccess)
+            g_ctx_get_current = reinterpret_cast<CtxGetCurrentFn>(fn);
+        fn = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &fn, cudaEnableDefault, &found) == cudaSuccess &&
+            found == cudaDriverEntryPointSuccess)
+            g_ctx_get_id = reinterpret_cast<CtxGetIdFn>(fn);
+        cudaGetLastError();  // a failed query leaves no error behind for the next launch
+    });
+    if (!g_ctx_get_current || !g_ctx_get_id) return 0;
+    void* ctx = nullptr;
+    unsigned long long id = 0;
+    if (g_ctx_get_current(&ctx) != 0 || !ctx || g_ctx_get_id(ctx, &id) != 0) return 0;
+    return id;
+}
+
 // Bits the kernels raise when a bounded wait gives up (one word per device).
 static __device__ unsigned g_device_errors;
 
+// The word's device address, looked up with cudaGetSymbolAddress once per device and
+// context (with that device current) and kept with the context's identity; a new context
+// (after cudaDeviceReset) or an unknown identity looks it up again. Safe to call from
+// several host threads.
 unsigned* device_error_word() {
     int device = 0;
     if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= 64) return nullptr;
+    static std::mutex lock;
+    static unsigned long long owner[64] = {0};
     static unsigned* words[64] = {nullptr};
-    if (!words[device]) {
+    std::lock_guard<std::mutex> guard(lock);
+    const unsigned long long ctx = current_context_id();
+    if (!words[device] || ctx == 0 || owner[device] != ctx) {
         void* p = nullptr;
         if (record_cuda_error(cudaGetSymbolAddress(&p, g_device_errors)) != MPF_OK) return nullptr;
         words[device] = static_cast<unsigned*>(p);
+        owner[device] = current_context_id();
     }
     return words[device];
 }
@@ -112,13 +150,14 @@ static int check_rows(const void* p, int64_t& stride, int64_t n, int rows, int d
 }
 
 static Tuning tuning_of(const mpf_tuning* t) {
-    Tuning u{0, 0, 0, 0, 0};
+    Tuning u{0, 0, 0, 0, 0, 0};
     if (t) {
         u.variant = t->variant;
         u.path = t->path;
         u.block = t->block;
         u.smem_bytes = t->smem_bytes;
         u.ctas_per_sm = t->ctas_per_sm;
+        u.wait_limit = t->wait_limit;
     }
     return u;
 }
@@ -527,11 +566,16 @@ int mpf_sort_workspace_bytes(int64_t n, int64_t num_tiles, size_t* bytes) {
     return MPF_OK;
 }
 
-int mpf_sort_by_tile(int kind, int degree, int ndim, const void* positions, int64_t pos_stride, const void* values,
-                     int64_t val_stride, int64_t ncomp, int64_t n, const double* lower, const double* cell,
-                     const int32_t* num, const int32_t* code, const int32_t* tile, int within, uint32_t* keys,
-                     int32_t* order, int64_t* tile_start, void* workspace, size_t workspace_bytes, int dtype,
-                     void* stream) {
+}  // extern "C"
+namespace mpf {
+// The argument checks of mpf_sort_by_tile apart from its workspace (shared with
+// mpf_sort_by_tile_noalloc, which checks them before any CUDA call); a row stride of 0
+// becomes n, and the number of tiles and the cells per tile key unit are set.
+int check_sort_arguments(int kind, int degree, int ndim, const void* positions, int64_t& pos_stride,
+                         const void* values, int64_t& val_stride, int64_t ncomp, int64_t n, const double* lower,
+                         const double* cell, const int32_t* num, const int32_t* code, const int32_t* tile,
+                         int within, const uint32_t* keys, const int32_t* order, const int64_t* tile_start,
+                         int dtype, int64_t* ntiles_out, int64_t* cells_out) {
     if (!valid_kind(kind, degree) || (dtype != MPF_F64 && dtype != MPF_F32)) return MPF_ERR_ARGUMENT;
     MPF_TRY(check_grid(kind, degree, ndim, lower, cell, num, code));
     if (n < 0 || n > INT32_MAX) return MPF_ERR_ARGUMENT;
@@ -548,6 +592,22 @@ int mpf_sort_by_tile(int kind, int degree, int ndim, const void* positions, int6
         MPF_TRY(check_rows(values, val_stride, n, (int)ncomp, dtype));
     }
     if (!tile_start || (n > 0 && (!keys || !order))) return MPF_ERR_ARGUMENT;
+    *ntiles_out = ntiles;
+    *cells_out = cells;
+    return MPF_OK;
+}
+
+}  // namespace mpf
+extern "C" {
+
+int mpf_sort_by_tile(int kind, int degree, int ndim, const void* positions, int64_t pos_stride, const void* values,
+                     int64_t val_stride, int64_t ncomp, int64_t n, const double* lower, const double* cell,
+                     const int32_t* num, const int32_t* code, const int32_t* tile, int within, uint32_t* keys,
+                     int32_t* order, int64_t* tile_start, void* workspace, size_t workspace_bytes, int dtype,
+                     void* stream) {
+    int64_t ntiles = 0, cells = 1;
+    MPF_TRY(check_sort_arguments(kind, degree, ndim, positions, pos_stride, values, val_stride, ncomp, n, lower,
+                                 cell, num, code, tile, within, keys, order, tile_start, dtype, &ntiles, &cells));
     if (workspace_bytes < sort_workspace_bytes(n) || (!workspace && n > 0)) return MPF_ERR_WORKSPACE;
     if ((reinterpret_cast<uintptr_t>(workspace) % 256) != 0) return MPF_ERR_ALIGNMENT;
     const cudaStream_t s = static_cast<cudaStream_t>(stream);

@@ -35,12 +35,17 @@ template <typename T> struct NodeArgs {
     int force_global;    // 1: never stage (the direct path), for tests and unsorted input
     int bulk;            // 1: positions are 16-byte aligned rows, prefetched by bulk copies
     unsigned* error;     // device word of MPF_DEVICE_ERROR_* bits
+    int wait_limit;      // tries of a bounded wait before it gives up (0: gives up at once)
     // a scatter of markers sorted by cell tile (mpf_sort_by_tile); tile_start null otherwise
     const int64_t* tile_start;  // first rank of every tile, then of the sentinel tile
     int64_t ntiles;
     int tile[3];         // anchor nodes per tile, per axis
     int tiles[3];        // tiles per axis
 };
+
+// The tries of a bounded wait on a bulk copy before a CTA gives up (about 0.1 s of
+// polling): far beyond any copy of a working device.
+constexpr int kDefaultWaitLimit = 1 << 22;
 
 // The tuning of one launch (the autotuned table supplies it; zero fields take defaults).
 struct Tuning {
@@ -49,6 +54,7 @@ struct Tuning {
     int smem_bytes;  // dynamic shared memory per CTA for the box
     int ctas_per_sm; // resident CTAs per SM the grid is sized for
     int variant;     // kernel variant, 0 the default for the shape
+    int wait_limit;  // tries of a bounded wait: 0 the default, < 0 none (gives up at once)
 };
 
 template <typename T, int NDIM>
@@ -121,6 +127,12 @@ int unpermute_rows(void* dst, int64_t ds, const void* src, int64_t ss, int64_t r
                    int64_t n, int dtype, cudaStream_t stream);
 
 int sm_count();
+
+int check_sort_arguments(int kind, int degree, int ndim, const void* positions, int64_t& pos_stride,
+                         const void* values, int64_t& val_stride, int64_t ncomp, int64_t n, const double* lower,
+                         const double* cell, const int32_t* num, const int32_t* code, const int32_t* tile,
+                         int within, const uint32_t* keys, const int32_t* order, const int64_t* tile_start,
+                         int dtype, int64_t* ntiles_out, int64_t* cells_out);
 }  // namespace mpf
 struct mpf_batch_request;
 struct mpf_batch_header;
@@ -138,6 +150,12 @@ void count_launches(int k);
 
 // The device word the kernels report MPF_DEVICE_ERROR_* bits in (per device), or NULL.
 unsigned* device_error_word();
+
+// A number that identifies the CUDA context current on the calling thread (the driver's
+// cuCtxGetId), or 0 when there is none or the driver does not tell. Addresses of
+// __device__ variables are cached per device and per this identity, so that a cache
+// never outlives its context (cudaDeviceReset makes a new one).
+unsigned long long current_context_id();
 
 // MPF_OK after a launch, or MPF_ERR_CUDA with the CUDA error recorded for mpf_last_error.
 int launch_status();

@@ -297,7 +297,6 @@ __device__ __forceinline__ void chunk_range(int64_t nchunks, int64_t& first, int
 // copies (cp.async.bulk, no multicast) completing on an mbarrier; every wait is bounded
 // and a CTA that gives up records MPF_DEVICE_ERROR_WAIT in *a.error and leaves.
 
-constexpr int kWaitLimit = 1 << 22;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -318,8 +317,8 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
 
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
-    for (int i = 0; i < kWaitLimit; ++i) {
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, int limit) {
+    for (int i = 0; i < limit; ++i) {
         uint32_t done;
         asm volatile(
             "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
@@ -344,6 +343,18 @@ __device__ __forceinline__ void issue_positions(const NodeArgs<T>& a, T* buf, in
     for (int j = bulk / sizeof(T); j < count; ++j)
 #pragma unroll
         for (int d = 0; d < NDIM; ++d) buf[d * CH + j] = a.pos[d * a.pos_stride + first + j];
+}
+
+// A CTA that gave up waiting for the positions of its chunk k (buffer b): before it
+// leaves, thread 0 waits for every bulk copy it issued that may still be in flight -- the
+// one into buffer b and, if issued, the next chunk's into buffer b ^ 1 -- each wait
+// bounded by the default limit, so that no copy lands in shared memory after the CTA
+// has handed it back. Then it records MPF_DEVICE_ERROR_WAIT.
+template <typename T>
+__device__ __forceinline__ void drain_and_flag(const NodeArgs<T>& a, uint64_t* bars, int b, int k, bool next) {
+    mbar_wait(&bars[b], (k >> 1) & 1, kDefaultWaitLimit);
+    if (next) mbar_wait(&bars[b ^ 1], ((k + 1) >> 1) & 1, kDefaultWaitLimit);
+    atomicOr(a.error, (unsigned)MPF_DEVICE_ERROR_WAIT);
 }
 
 template <typename T>
@@ -390,11 +401,9 @@ __global__ void __launch_bounds__(kMaxBlock, 2) gather_kernel(const NodeArgs<T> 
                 issue_positions<T, NDIM>(a, posbuf + (b ^ 1) * NDIM * CH, CH, first + CH,
                                          (int)min((int64_t)CH, a.n - first - CH), &bars[b ^ 1]);
             }
-            const bool late = !mbar_wait(&bars[b], (k >> 1) & 1);
+            const bool late = !mbar_wait(&bars[b], (k >> 1) & 1, a.wait_limit);
             if (__syncthreads_or(late)) {
-                if (threadIdx.x == 0) atomicOr(a.error, (unsigned)MPF_DEVICE_ERROR_WAIT);
-                // the copy that may still be in flight lands in this CTA's own buffer
-                if (threadIdx.x == 0 && ci + 1 < c_last) mbar_wait(&bars[b ^ 1], ((k + 1) >> 1) & 1);
+                if (threadIdx.x == 0) drain_and_flag(a, bars, b, k, ci + 1 < c_last);
                 __syncthreads();
                 return;
             }
@@ -550,10 +559,9 @@ __global__ void __launch_bounds__(kMaxBlock, MINB) gather_l1_kernel(const NodeAr
                 issue_positions<T, NDIM>(a, posbuf + (b ^ 1) * NDIM * CH, CH, first + CH,
                                          (int)min((int64_t)CH, a.n - first - CH), &bars[b ^ 1]);
             }
-            const bool late = !mbar_wait(&bars[b], (k >> 1) & 1);
+            const bool late = !mbar_wait(&bars[b], (k >> 1) & 1, a.wait_limit);
             if (__syncthreads_or(late)) {
-                if (threadIdx.x == 0) atomicOr(a.error, (unsigned)MPF_DEVICE_ERROR_WAIT);
-                if (threadIdx.x == 0 && ci + 1 < c_last) mbar_wait(&bars[b ^ 1], ((k + 1) >> 1) & 1);
+                if (threadIdx.x == 0) drain_and_flag(a, bars, b, k, ci + 1 < c_last);
                 __syncthreads();
                 return;
             }

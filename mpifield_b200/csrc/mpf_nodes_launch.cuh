@@ -120,6 +120,7 @@ static int run_gather(NodeArgs<T> a, const Tuning& t, cudaStream_t stream) {
     a.bulk = bulk_positions<T, NDIM>(a);
     a.error = device_error_word();
     if (!a.error) return MPF_ERR_CUDA;
+    a.wait_limit = t.wait_limit == 0 ? kDefaultWaitLimit : std::max(t.wait_limit, 0);
     const int64_t nchunks = (a.n + CH - 1) / CH;
     if (l1) {
         // (the boundary codes stay run-time values here: a periodic-only build of this kernel

@@ -11,6 +11,7 @@
 // the result is the stable order (numpy.argsort(keys, kind="stable")), bit for bit.
 #include <algorithm>
 #include <cstdint>
+#include <mutex>
 
 #include "mpf_internal.h"
 #include "mpf_stencil.cuh"
@@ -405,28 +406,39 @@ int unpermute_rows(void* dst, int64_t ds, const void* src, int64_t ss, int64_t r
 
 // ------------------------------------------------- the sort without allocation --
 //
-// Callers that cannot call cudaMalloc -- code recorded into a CUDA graph, where an
-// allocation may not be captured; a host application that owns every byte of device
-// memory through its own pool; a real-time loop that must not take the implicit device
-// synchronisation of an allocation -- sort through mpf_sort_by_tile_noalloc, whose
-// workspace is this file-scope array: every GPU that loads the library holds it (about
-// 18 MB) until the process exits, it keeps the last call's contents, and calls that
-// overlap on the GPU (two streams at once) race on it.
+// Some callers of the sort cannot call cudaMalloc: a host application that hands every
+// byte of device memory to its own pool or arena at start-up and allows no allocation
+// afterwards, or a real-time loop (a control or streaming step) that cannot take the
+// implicit device synchronisation an allocation may bring. They sort through
+// mpf_sort_by_tile_noalloc, whose workspace is this file-scope array instead of a buffer
+// of theirs: every GPU that loads the library holds it (sort_layout(2^20).total, about
+// 18 MB) until the process exits; it keeps the last call's contents (no part of the sort
+// needs a starting value in it: every pass writes what it later reads); and calls that
+// overlap on the GPU (on two streams, or from two host threads at once) race on it.
 
 constexpr int64_t kNoAllocMaxMarkers = MPF_NOALLOC_MAX_MARKERS;
 constexpr size_t kNoAllocBytes = sort_layout(kNoAllocMaxMarkers).total;
 
 static __device__ __align__(256) unsigned char g_noalloc_sort_scratch[kNoAllocBytes];
 
-// The device address of the array on the current device, looked up once per device.
+// The device address of the array on the current device. In host code the array's name
+// stands for a host-side shadow, not device memory, so kernels get this address instead:
+// cudaGetSymbolAddress with the device current, once per device and context (kept with
+// the context's identity, looked up again in a new context, e.g. after cudaDeviceReset),
+// under a lock so that host threads may call concurrently. Null on a CUDA error.
 static void* noalloc_scratch() {
     int device = 0;
-    if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= 64) return nullptr;
+    if (record_cuda_error(cudaGetDevice(&device)) != MPF_OK || device < 0 || device >= 64) return nullptr;
+    static std::mutex lock;
+    static unsigned long long owner[64] = {0};
     static void* address[64] = {nullptr};
-    if (!address[device]) {
+    std::lock_guard<std::mutex> guard(lock);
+    const unsigned long long ctx = current_context_id();
+    if (!address[device] || ctx == 0 || owner[device] != ctx) {
         void* p = nullptr;
         if (record_cuda_error(cudaGetSymbolAddress(&p, g_noalloc_sort_scratch)) != MPF_OK) return nullptr;
         address[device] = p;
+        owner[device] = current_context_id();
     }
     return address[device];
 }
@@ -441,11 +453,17 @@ extern "C" int mpf_sort_by_tile_noalloc(int kind, int degree, int ndim, const vo
                                         const double* lower, const double* cell, const int32_t* num,
                                         const int32_t* code, const int32_t* tile, int within, uint32_t* keys,
                                         int32_t* order, int64_t* tile_start, int dtype, void* stream) {
-    // more markers than the array holds: refused before any device work
+    // every argument is checked before any CUDA call: a bad one returns its status and
+    // touches neither the device nor the array
+    if (n < 0) return MPF_ERR_ARGUMENT;
     if (n > mpf::kNoAllocMaxMarkers) return MPF_ERR_WORKSPACE;
+    int64_t ntiles = 0, cells = 1;
+    const int checked = mpf::check_sort_arguments(kind, degree, ndim, positions, pos_stride, values, val_stride,
+                                                  ncomp, n, lower, cell, num, code, tile, within, keys, order,
+                                                  tile_start, dtype, &ntiles, &cells);
+    if (checked != MPF_OK) return checked;
     void* scratch = mpf::noalloc_scratch();
     if (!scratch) return MPF_ERR_CUDA;
-    // no entry of the workspace needs a starting value: every pass writes what it reads
     return mpf_sort_by_tile(kind, degree, ndim, positions, pos_stride, values, val_stride, ncomp, n, lower, cell,
                             num, code, tile, within, keys, order, tile_start, scratch, mpf::kNoAllocBytes, dtype,
                             stream);

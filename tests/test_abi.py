@@ -94,6 +94,29 @@ def test_invalid_arguments_return_a_status_before_any_device_work():
                                 fake, 16, 0, None) == _lib.ERR_WORKSPACE
 
 
+def test_the_sort_without_allocation_checks_everything_before_any_cuda_call():
+    # no CUDA device here: a call that reached the device would return MPF_ERR_CUDA
+    lib = _lib.library()
+    lower, cell, num, code = _geom()
+    t = (C.c_int32 * 3)(4, 4, 4)
+    fake = 1 << 20  # never dereferenced
+    most = 1 << 20  # MPF_NOALLOC_MAX_MARKERS
+
+    def call(n=1000, kind=1, degree=2, ndim=3, pos=fake, within=0, dtype=0, order=fake):
+        return lib.mpf_sort_by_tile_noalloc(kind, degree, ndim, pos, 0, None, 0, 0, n, lower, cell, num, code, t,
+                                            within, fake, order, fake, dtype, None)
+
+    assert call(n=most + 1) == _lib.ERR_WORKSPACE
+    assert call(n=-1) == _lib.ERR_ARGUMENT
+    assert call(kind=0) == _lib.ERR_ARGUMENT  # LINEAR is degree 1
+    assert call(ndim=4) == _lib.ERR_ARGUMENT
+    assert call(within=2) == _lib.ERR_ARGUMENT
+    assert call(dtype=5) == _lib.ERR_ARGUMENT
+    assert call(pos=fake + 3) == _lib.ERR_ALIGNMENT
+    assert call(order=0) == _lib.ERR_ARGUMENT
+    assert lib.mpf_last_error() == b"none"
+
+
 def test_tile_counts_and_workspace_sizes():
     lib = _lib.library()
     num = (C.c_int32 * 3)(256, 256, 256)

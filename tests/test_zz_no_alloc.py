@@ -1,13 +1,14 @@
 """The allocation-free sort entry point (mpf_sort_by_tile_noalloc), through the C ABI.
 
-Some callers cannot allocate device memory: work recorded into a CUDA graph, a host
-application that owns all device memory through its own pool, a real-time loop that
-cannot afford an allocation's implicit synchronisation. For them the library sorts in a
-fixed array of its own instead of a caller's workspace. This test checks that two calls
-in a row (the array keeps the previous call's contents) give exactly the keys, order and
-tile starts of mpf_sort_by_tile with a workspace of its own, and that a size above the
-array's limit is refused. It lives in a file of its own, collected last, so that a run
-stopping at the first failure has run every other test first.
+Some callers cannot call cudaMalloc: a host application that gives all device memory to
+its own pool at start-up, a real-time loop that cannot afford an allocation's implicit
+synchronisation. For them the library sorts in a fixed array of its own instead of a
+caller's workspace. This test checks that two calls in a row (the array keeps the
+previous call's contents) give exactly the keys, order and tile starts of
+mpf_sort_by_tile with a workspace of its own. (Sizes above the array's limit and bad
+arguments are refused before any CUDA call; tests/test_abi.py checks that without a
+GPU.) It lives in a file of its own, collected last, so that a run stopping at the
+first failure has run every other test first.
 """
 
 from __future__ import annotations
@@ -76,12 +77,3 @@ def test_two_calls_in_a_row_match_the_sort_with_a_workspace():
         got = _sort(positions, values, within, noalloc=True)
         for a, b in zip(got, expected):
             np.testing.assert_array_equal(a, b)
-
-
-def test_more_markers_than_the_array_holds_are_refused():
-    lib = _lib.library()
-    lower, cell, num, code, tile = _geometry()
-    fake = 1 << 20  # never dereferenced: the size check comes first
-    status = lib.mpf_sort_by_tile_noalloc(1, 2, 3, fake, 0, None, 0, 0, MAX_MARKERS + 1, lower, cell, num, code,
-                                          tile, 0, fake, fake, fake, _lib.F64, None)
-    assert status == _lib.ERR_WORKSPACE
