@@ -3,11 +3,13 @@
 B-spline gather and scatter of degree 0-3 in 1D-3D (`LINEAR`, `QUADRATIC`, `CUBIC`), the
 charge-conserving path deposit (`WHITNEY`, `QUADRATIC_EDGES`, `CUBIC_EDGES`) and the
 single-GPU halo fill and fold-back, behind mpifield's `Weighting` / `EdgeWeighting`
-kernel convention and a `Field` with its gather / scatter / deposit_density; torch
-tensors on a CUDA device, hand-written sm_100a kernels through the C ABI of
+kernel convention and a `Field` with its gather / scatter / deposit_density; device
+arrays of any producer (CuPy, torch, ``__cuda_array_interface__``, DLPack) on the
+caller's stream, hand-written sm_100a kernels through the C ABI of
 ``include/mpifield_b200.h`` (``libmpifield_b200.so``). There is no CPU fallback.
 """
 
+from mpifield_b200._arrays import use_stream
 from mpifield_b200._types import BlockGrid, Bounds
 from mpifield_b200.edges import CUBIC_EDGES, QUADRATIC_EDGES, WHITNEY, EdgeWeighting
 from mpifield_b200.field import Field
@@ -19,6 +21,6 @@ from mpifield_b200.weighting import CUBIC, LINEAR, QUADRATIC, Weighting, spline_
 __all__ = [
     "BlockGrid", "Bounds", "CLAMPED_SPLINES", "CUBIC", "CUBIC_EDGES", "EdgeWeighting", "Field", "KERNELS",
     "LINEAR", "QUADRATIC", "QUADRATIC_EDGES", "SPLINES", "Splines", "TileOrder", "WHITNEY", "Weighting",
-    "permute", "sort_by_tile", "spline_weighting", "splines", "unpermute",
+    "permute", "sort_by_tile", "spline_weighting", "splines", "unpermute", "use_stream",
 ]
 __version__ = "1.0.0"

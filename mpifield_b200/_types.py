@@ -1,31 +1,69 @@
-"""`BlockGrid`: the grid of a block as the kernels see it.
+"""The grid of a block as the kernels see it: `Bounds` and `BlockGrid`.
 
-The same value type as mpifield's ``BlockGrid`` (src/mpifield/_types.py:27-96): bounds,
-spacing, node counts, periodic and clamped flags, and ``geometry``, the kernels' trailing
-arguments ``(*lower, *cell_size, *num_nodes, *code)`` with code 0 bounded, 1 periodic,
-2 clamped.
+Code written against mpifield reads a grid through the fields of its ``BlockGrid``
+(src/mpifield/_types.py:27-96): the same names in the same order, and the same
+``from_geometry`` arguments and errors, are kept here. The grid is built from one
+`_Axis` record per axis; ``geometry`` is what the kernels take after their arrays,
+``(*lower, *cell_size, *num_nodes, *code)`` with the boundary codes 0 (bounded),
+1 (periodic) and 2 (clamped spline knots).
 """
 
 from __future__ import annotations
 
+from itertools import zip_longest
 from typing import NamedTuple
 
 import numpy as np
 
+BOUNDED, PERIODIC, CLAMPED = 0, 1, 2
+
 
 class Bounds(NamedTuple):
-    """The lower and upper corner of a grid block, one entry per axis."""
+    """Positions of a block's first node (``lower_bound``) and last node (``upper_bound``)
+    along every axis."""
 
     lower_bound: np.ndarray
     upper_bound: np.ndarray
 
 
-class BlockGrid(NamedTuple):
-    """The grid of a block (halo nodes included), for the kernels.
+class _Axis(NamedTuple):
+    """One axis of a grid: first node, spacing, node count and boundary code."""
 
-    ``geometry`` is ``(*lower, *cell_size, *num_nodes, *code)``; ``index`` selects the
-    nodes of the grid in a field's ``local_with_halos``; ``clamped`` marks the axes with
-    clamped spline knots, where an array of degree p holds ``num_nodes + p - 1`` entries.
+    first: float
+    step: float
+    count: int
+    code: int
+
+    @property
+    def last(self) -> float:
+        return self.first + (self.count - 1) * self.step
+
+
+def _flags(values, ndim: int) -> tuple[bool, ...]:
+    return (False,) * ndim if values is None else tuple(bool(v) for v in values)
+
+
+def _axes(lower, cell_size, num_nodes, periodic, clamped) -> list[_Axis]:
+    counts = [int(n) for n in num_nodes]
+    ndim = len(counts)
+    rows = list(zip_longest(lower, cell_size, counts, _flags(periodic, ndim), _flags(clamped, ndim)))
+    if any(None in row for row in rows):
+        raise ValueError("lower, cell_size, num_nodes, periodic and clamped differ in length")
+    axes = []
+    for first, step, count, wraps, knots in rows:
+        if wraps and knots:
+            raise ValueError("an axis is either periodic or clamped")
+        code = CLAMPED if knots else (PERIODIC if wraps else BOUNDED)
+        axes.append(_Axis(float(first), float(step), count, code))
+    return axes
+
+
+class BlockGrid(NamedTuple):
+    """The nodes of a block, halo nodes included, as the kernels address them.
+
+    ``geometry`` is the kernels' trailing arguments; ``index`` picks the grid's nodes out
+    of a stored array with halos; ``clamped`` flags the axes with clamped spline knots,
+    along which an array of degree p holds ``num_nodes + p - 1`` coefficients.
     """
 
     bounds: Bounds
@@ -38,27 +76,17 @@ class BlockGrid(NamedTuple):
 
     @classmethod
     def from_geometry(cls, lower, cell_size, num_nodes, periodic=None, clamped=None) -> BlockGrid:
-        """The grid of a whole array of ``num_nodes`` nodes from ``lower`` on."""
-        lower = tuple(float(v) for v in lower)
-        cell_size = tuple(float(v) for v in cell_size)
-        num_nodes = tuple(int(n) for n in num_nodes)
-        ndim = len(num_nodes)
-        flags = (False,) * ndim if periodic is None else tuple(map(bool, periodic))
-        ends = (False,) * ndim if clamped is None else tuple(map(bool, clamped))
-        if not len(lower) == len(cell_size) == len(flags) == len(ends) == ndim:
-            raise ValueError("lower, cell_size, num_nodes, periodic and clamped differ in length")
-        if any(f and e for f, e in zip(flags, ends)):
-            raise ValueError("an axis is either periodic or clamped")
-        lower_bound = np.asarray(lower, dtype=float)
-        spacing = np.asarray(cell_size, dtype=float)
-        nodes = np.asarray(num_nodes, dtype=int)
-        codes = tuple(2 if end else int(flag) for flag, end in zip(flags, ends))
+        """The grid of a whole array: ``num_nodes`` nodes per axis from ``lower`` on,
+        ``cell_size`` apart; axes bounded unless ``periodic`` or ``clamped`` flags them."""
+        axes = _axes(lower, cell_size, num_nodes, periodic, clamped)
+        first = np.array([a.first for a in axes], dtype=float)
         return cls(
-            bounds=Bounds(lower_bound, lower_bound + (nodes - 1) * spacing),
-            grid_spacing=spacing,
-            num_gridpoints=nodes,
-            periodic=flags,
-            geometry=(*lower, *cell_size, *num_nodes, *codes),
-            index=(slice(None),) * ndim,
-            clamped=ends,
+            bounds=Bounds(first, np.array([a.last for a in axes], dtype=float)),
+            grid_spacing=np.array([a.step for a in axes], dtype=float),
+            num_gridpoints=np.array([a.count for a in axes], dtype=int),
+            periodic=tuple(a.code == PERIODIC for a in axes),
+            geometry=(*(a.first for a in axes), *(a.step for a in axes), *(a.count for a in axes),
+                      *(a.code for a in axes)),
+            index=tuple(slice(None) for _ in axes),
+            clamped=tuple(a.code == CLAMPED for a in axes),
         )

@@ -1,54 +1,62 @@
-"""Edge fields: the edge gather and the charge-conserving path deposit.
+"""Edge fields on the B200 kernels: `EdgeWeighting`, `WHITNEY`, `QUADRATIC_EDGES`, `CUBIC_EDGES`.
 
-The same plug-in type as mpifield's ``EdgeWeighting`` (src/mpifield/edges.py:98-265):
-``EdgeWeighting(name, gather={ndim: kernel}, deposit_paths={ndim: kernel}, halo, degree,
-clamps)`` with ``gather_block``, ``deposit_paths_block``, ``gradient_block`` and
-``divergence_block``, and the built-ins `WHITNEY` (degree 1), `QUADRATIC_EDGES` and
-`CUBIC_EDGES` on the sm_100a kernels. An edge field is ``num_nodes + (ndim,)``: entry
-``(k, a)`` the line integral along the edge from node k to its neighbour along axis a
-(``num_nodes + p - 1`` entries along a clamped axis).
+An edge field holds, for every node and axis, the line integral along the edge from the
+node to its neighbour along that axis: an array ``num_nodes + (ndim,)`` (``num_nodes +
+p - 1`` entries along a clamped axis of degree p). `EdgeWeighting` is mpifield's plug-in
+type for the two operations on it (src/mpifield/edges.py:98-265): ``EdgeWeighting(name,
+gather={ndim: kernel}, deposit_paths={ndim: kernel}, halo, degree, clamps)`` with
+`gather_block` (the field at markers) and `deposit_paths_block` (the current of charges
+moving along straight paths), and the discrete gradient `gradient_block` and its
+transpose `divergence_block`, with which the deposit conserves charge:
+``divergence_block(J)`` equals the node deposit at the paths' ends minus at their starts.
 """
 
 from __future__ import annotations
 
 from collections.abc import Callable, Mapping
 from dataclasses import dataclass
-from types import MappingProxyType
 from typing import Any
 
-import torch
-
 from mpifield_b200 import _lib
+from mpifield_b200._arrays import as_device_array
+from mpifield_b200._plugins import KernelTable, on_device_of
 from mpifield_b200._types import BlockGrid
 from mpifield_b200.kernels import EdgeGatherKernel, PathKernel
-from mpifield_b200.weighting import _as_marker_tensor, _check_clamps
 
 __all__ = ["CUBIC_EDGES", "QUADRATIC_EDGES", "WHITNEY", "EdgeWeighting"]
 
 KernelFunction = Callable[..., Any]
 
 
-def _checked(kernels: Mapping[int, KernelFunction], role: str) -> Mapping[int, Any]:
-    for ndim in kernels:
-        if ndim not in (1, 2, 3):
-            raise ValueError(f"{role} kernels are for 1, 2 or 3 dimensions, got {ndim}")
-    return MappingProxyType(dict(kernels))
+def _shift(t, axis: int, periodic: bool, toward_end: bool):
+    """``t`` moved one node along ``axis`` (toward the end or the start); on a bounded
+    axis the vacated entry is zero, on a periodic one it wraps."""
+    import torch
+
+    if periodic:
+        return torch.roll(t, 1 if toward_end else -1, dims=axis)
+    n = t.shape[axis]
+    zero = torch.zeros_like(t.narrow(axis, 0, 1))
+    if toward_end:
+        return torch.cat((zero, t.narrow(axis, 0, n - 1)), dim=axis)
+    return torch.cat((t.narrow(axis, 1, n - 1), zero), dim=axis)
 
 
-@dataclass(frozen=True)
-class _WithDegree:
-    """A spline edge kernel with its degree appended."""
-
-    kernel: KernelFunction
-    degree: int
-
-    def __call__(self, *arguments: Any) -> None:
-        self.kernel(*arguments, self.degree)
+def _last_node_cleared(t, axis: int):
+    """``t`` with its last node along ``axis`` zero (no edge leaves it on a bounded axis)."""
+    out = t.clone()
+    out.narrow(axis, t.shape[axis] - 1, 1).zero_()
+    return out
 
 
 @dataclass(frozen=True, eq=False, repr=False)
-class EdgeWeighting:
-    """The edge gather and its path deposit, for each number of dimensions they cover."""
+class EdgeWeighting(KernelTable):
+    """Edge gather and path-deposit kernels by number of dimensions, with the halo a split
+    field needs, the B-spline degree (1 for Whitney) and whether they take clamped axes."""
+
+    ROLES = ("gather", "deposit_paths")
+    NOUN = "edge weighting"
+    LOWEST_DEGREE = 1
 
     name: str
     gather: Mapping[int, KernelFunction]
@@ -57,112 +65,82 @@ class EdgeWeighting:
     degree: int | None = None
     clamps: bool = False
 
-    def __post_init__(self) -> None:
-        if self.halo < 0:
-            raise ValueError(f"halo must be >= 0, got {self.halo}")
-        if self.degree is not None and self.degree < 1:
-            raise ValueError(f"degree must be >= 1, got {self.degree}")
-        object.__setattr__(self, "gather", _checked(self.gather, "gather"))
-        object.__setattr__(self, "deposit_paths", _checked(self.deposit_paths, "deposit_paths"))
-
-    def _kernel(self, kernels, ndim: int, role: str):
-        try:
-            return kernels[ndim]
-        except KeyError:
-            have = ", ".join(f"{n}D" for n in sorted(kernels)) or "none"
-            raise ValueError(f"the {self.name} edge weighting has no {ndim}D {role} kernel (has {have})") from None
-
     def gather_kernel(self, ndim: int) -> KernelFunction:
-        return self._kernel(self.gather, ndim, "gather")
+        return self.kernel("gather", ndim)
 
     def deposit_paths_kernel(self, ndim: int) -> KernelFunction:
-        return self._kernel(self.deposit_paths, ndim, "deposit_paths")
+        return self.kernel("deposit_paths", ndim)
 
-    def _check(self, edges: torch.Tensor, grid: BlockGrid) -> int:
-        """The number of dimensions of ``grid``, checking the shape of ``edges``."""
-        _check_clamps(self, grid)
-        ndim = len(grid.periodic)
-        ends = grid.clamped or (False,) * ndim
-        extra = 0 if self.degree is None else self.degree - 1
-        expected = (*(int(n) + (extra if end else 0) for n, end in zip(grid.num_gridpoints, ends)), ndim)
-        if tuple(edges.shape) != expected:
-            raise ValueError(f"an edge field on this grid is {expected}, got {tuple(edges.shape)}")
+    def _edge_field_ndim(self, edges, grid: BlockGrid) -> int:
+        """The dimensions of ``grid``, after checking the shape of the edge field on it."""
+        ndim = self.accept_grid(grid)
+        extra = (self.degree or 1) - 1
+        clamped = grid.clamped or (False,) * ndim
+        want = tuple(int(n) + (extra if c else 0) for n, c in zip(grid.num_gridpoints, clamped)) + (ndim,)
+        have = as_device_array(edges, "edges").shape
+        if have != want:
+            raise ValueError(f"an edge field on this grid is {want}, got {have}")
         return ndim
 
-    def gather_block(self, positions, edges: torch.Tensor, result: torch.Tensor, grid: BlockGrid) -> None:
+    def gather_block(self, positions, edges, result, grid: BlockGrid) -> None:
         """Write the field of ``edges`` at ``positions`` (ndim, N) into ``result`` (ndim, N)."""
-        kernel = self.gather_kernel(self._check(edges, grid))
-        positions = _as_marker_tensor(positions, edges)
-        kernel(positions, edges, result, *grid.geometry)
+        run = self.gather_kernel(self._edge_field_ndim(edges, grid))
+        run(on_device_of(positions, edges), edges, result, *grid.geometry)
 
-    def deposit_paths_block(self, start, end, charges, edges: torch.Tensor, grid: BlockGrid) -> None:
-        """Add the current of ``charges`` (N,) moving from ``start`` to ``end`` (ndim, N) to ``edges``."""
-        kernel = self.deposit_paths_kernel(self._check(edges, grid))
-        start = _as_marker_tensor(start, edges)
-        end = _as_marker_tensor(end, edges)
-        charges = _as_marker_tensor(charges, edges).reshape(-1)
-        if start.shape != end.shape or start.shape[-1] != charges.shape[0]:
-            raise ValueError(
-                f"paths from {tuple(start.shape)} to {tuple(end.shape)} for {charges.shape[0]} charges"
-            )
-        kernel(start, end, charges, edges, *grid.geometry)
+    def deposit_paths_block(self, start, end, charges, edges, grid: BlockGrid) -> None:
+        """Add to ``edges`` the current of ``charges`` (N,) moving in straight lines from
+        ``start`` to ``end`` (ndim, N)."""
+        run = self.deposit_paths_kernel(self._edge_field_ndim(edges, grid))
+        start, end, charges = (on_device_of(a, edges) for a in (start, end, charges))
+        s, e, q = (as_device_array(a) for a in (start, end, charges))
+        if s.shape != e.shape or s.shape[-1] != q.size:
+            raise ValueError(f"paths from {s.shape} to {e.shape} for {q.size} charges")
+        run(start, end, charges, edges, *grid.geometry)
 
     @staticmethod
-    def gradient_block(nodes: torch.Tensor, grid: BlockGrid) -> torch.Tensor:
-        """``G phi``: the difference of a node field along every edge (zero past a bounded end)."""
-        ndim = len(grid.periodic)
-        result = torch.zeros((*nodes.shape, ndim), dtype=nodes.dtype, device=nodes.device)
+    def gradient_block(nodes, grid: BlockGrid):
+        """``G phi`` (torch): every edge gets the difference of ``nodes`` between its end
+        and its start node; edges that leave a bounded axis at its last node get zero."""
+        import torch
+
+        nodes = as_device_array(nodes, "nodes").torch()
+        parts = []
         for axis, periodic in enumerate(grid.periodic):
-            if periodic:
-                result[..., axis] = torch.roll(nodes, -1, dims=axis) - nodes
-            else:
-                n = nodes.shape[axis]
-                result[..., axis].narrow(axis, 0, n - 1).copy_(
-                    nodes.narrow(axis, 1, n - 1) - nodes.narrow(axis, 0, n - 1))
-        return result
+            step = _shift(nodes, axis, periodic, toward_end=False) - nodes
+            parts.append(step if periodic else _last_node_cleared(step, axis))
+        return torch.stack(parts, dim=-1)
 
     @staticmethod
-    def divergence_block(edges: torch.Tensor, grid: BlockGrid) -> torch.Tensor:
-        """``G^T j``: the transpose of `gradient_block` (the change of the node charge)."""
-        result = torch.zeros(edges.shape[:-1], dtype=edges.dtype, device=edges.device)
+    def divergence_block(edges, grid: BlockGrid):
+        """``G^T j`` (torch), the transpose of `gradient_block`: every node gets what its
+        incoming edges carry minus what its outgoing edges carry -- the change of the
+        node charge the current brings."""
+        edges = as_device_array(edges, "edges").torch()
+        total = None
         for axis, periodic in enumerate(grid.periodic):
             flow = edges[..., axis]
-            if periodic:
-                result += torch.roll(flow, 1, dims=axis) - flow
-            else:
-                n = flow.shape[axis]
-                result.narrow(axis, 0, n - 1).sub_(flow.narrow(axis, 0, n - 1))
-                result.narrow(axis, 1, n - 1).add_(flow.narrow(axis, 0, n - 1))
-        return result
-
-    def __repr__(self) -> str:
-        dims = sorted(set(self.gather) | set(self.deposit_paths))
-        degree = "" if self.degree is None else f", degree={self.degree}"
-        return f"EdgeWeighting({self.name!r}, ndim={tuple(dims)}, halo={self.halo}{degree})"
+            if not periodic:
+                flow = _last_node_cleared(flow, axis)
+            term = _shift(flow, axis, periodic, toward_end=True) - flow
+            total = term if total is None else total + term
+        return total
 
 
-#: The lowest-order edge (Whitney) gather and path deposit, whose node space is LINEAR's.
-WHITNEY = EdgeWeighting(
-    "whitney",
-    gather={n: EdgeGatherKernel(_lib.LINEAR, n, False) for n in (1, 2, 3)},
-    deposit_paths={n: PathKernel(_lib.LINEAR, n, False) for n in (1, 2, 3)},
-    halo=1,
-    degree=1,
-)
+def _edge_tables(kind: int, degree: int) -> tuple[dict, dict]:
+    return ({n: EdgeGatherKernel(kind, n, False, degree) for n in (1, 2, 3)},
+            {n: PathKernel(kind, n, False, degree) for n in (1, 2, 3)})
 
 
-def _spline_edges(name: str, degree: int) -> EdgeWeighting:
-    return EdgeWeighting(
-        name,
-        gather={n: _WithDegree(EdgeGatherKernel(_lib.SPLINE, n, True), degree) for n in (1, 2, 3)},
-        deposit_paths={n: _WithDegree(PathKernel(_lib.SPLINE, n, True), degree) for n in (1, 2, 3)},
-        halo=2,
-        degree=degree,
-        clamps=True,
-    )
+def spline_edges(name: str, degree: int) -> EdgeWeighting:
+    """The spline edge weighting of degree 1-3 (along an edge degree - 1, across it
+    degree), on the spline-edge kernels; takes clamped axes."""
+    gather, deposit = _edge_tables(_lib.SPLINE, degree)
+    return EdgeWeighting(name, gather=gather, deposit_paths=deposit, halo=2, degree=degree, clamps=True)
 
 
-#: The edge weighting that goes with QUADRATIC (linear along an edge, quadratic across).
-QUADRATIC_EDGES = _spline_edges("quadratic", 2)
-#: The edge weighting that goes with CUBIC (quadratic along an edge, cubic across).
-CUBIC_EDGES = _spline_edges("cubic", 3)
+#: The lowest-order (Whitney) edges, whose node space is LINEAR's.
+WHITNEY = EdgeWeighting("whitney", *_edge_tables(_lib.LINEAR, 1), halo=1, degree=1)
+#: The edges that go with QUADRATIC (linear along an edge, quadratic across).
+QUADRATIC_EDGES = spline_edges("quadratic", 2)
+#: The edges that go with CUBIC (quadratic along an edge, cubic across).
+CUBIC_EDGES = spline_edges("cubic", 3)

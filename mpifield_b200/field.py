@@ -21,9 +21,17 @@ import torch
 
 from mpifield_b200 import _lib
 from mpifield_b200._types import BlockGrid, Bounds
-from mpifield_b200.weighting import LINEAR, Weighting, _as_marker_tensor
+from mpifield_b200.weighting import LINEAR, Weighting
 
 __all__ = ["Field"]
+
+
+def _markers_on(array, like: torch.Tensor) -> torch.Tensor:
+    """A marker array as a torch tensor on ``like``'s device in its dtype (no copy when it
+    is one already; device arrays of other producers are viewed, host arrays copied)."""
+    if isinstance(array, torch.Tensor):
+        return array if (array.device, array.dtype) == (like.device, like.dtype) else array.to(like.device, like.dtype)
+    return torch.as_tensor(array, dtype=like.dtype, device=like.device)
 
 
 def _per_axis(value, ndim: int, name: str) -> tuple:
@@ -130,7 +138,7 @@ class Field:
     # --------------------------------------------------------- gather / scatter --
 
     def _marker_positions(self, positions) -> torch.Tensor:
-        positions = _as_marker_tensor(positions, self.local_with_halos)
+        positions = _markers_on(positions, self.local_with_halos)
         if positions.dim() == 1:
             if self.ndim == 1:
                 return positions.reshape(1, -1)
@@ -144,7 +152,7 @@ class Field:
     def _marker_values(self, values, count: int) -> torch.Tensor:
         if isinstance(values, (int, float)):
             return torch.full((self.num_components, count), float(values), dtype=self.dtype, device=self.device)
-        values = _as_marker_tensor(values, self.local_with_halos)
+        values = _markers_on(values, self.local_with_halos)
         if values.dim() == 1:
             if values.shape[0] == count:
                 values = values.reshape(1, count)

@@ -8,17 +8,22 @@ src/mpifield/edges.py:23-31)::
     deposit_paths(start, end, charges, edges, *geometry)        # adds into edges
 
 with ``geometry = (*lower, *cell_size, *num_nodes, *code)`` and, for the spline kernels,
-a trailing ``degree``. The callables here take the same arguments as torch tensors on a
-CUDA device (float64, or float32 for the single-precision variant) and launch the
-sm_100a kernels of ``libmpifield_b200.so`` on torch's current stream, asynchronously.
-`KERNELS` maps the reference's kernel names (src/mpifield/kernels/catalog.py:51-93) to
-them; the linear 1D deposit also takes the reference's ``(N,)`` single-component arrays
-and the linear 3D kernels its ``(nx * ny * nz, ncomp)`` row fields.
+a trailing ``degree``. The callables here take the same arguments as device arrays --
+CuPy arrays as mpifield passes them, torch tensors, anything with
+``__cuda_array_interface__`` or ``__dlpack__`` (`_arrays`) -- in float64, or float32 for
+the single-precision variant, and launch the sm_100a kernels of ``libmpifield_b200.so``
+asynchronously on the caller's stream (`_arrays.launch_stream`). `KERNELS` maps the
+reference's kernel names (src/mpifield/kernels/catalog.py:51-93) to them, with the
+signatures the reference's catalog documents: the linear 1D deposit also takes one
+component as ``(N,)`` markers and an ``(nx,)`` grid, and the linear 3D kernels the grid
+as rows ``(nx * ny * nz, ncomp)`` (src/mpifield/weighting.py:259-330); the launch
+keywords the reference gives its CUDA kernels (``shared_mem``, ``n_threads``) are
+accepted and left to this backend's own launch configuration.
 
 Marker arrays are ``(rows, N)`` with a unit column stride and any row stride
-(``storage[:, :n]``); a copy is made only for other layouts (or another dtype), and a
-non-contiguous output is written through a contiguous copy, as
-``cunumpy.kernels.kernel_output`` does for the reference.
+(``storage[:, :n]``) and are passed as they are; another layout or element type is
+copied first, and an output the C calls cannot write in place is written through a
+contiguous copy, as ``cunumpy.kernels.kernel_output`` does for the reference.
 """
 
 from __future__ import annotations
@@ -26,59 +31,145 @@ from __future__ import annotations
 import ctypes as C
 from dataclasses import dataclass
 
-import torch
-
 from mpifield_b200 import _lib
+from mpifield_b200._arrays import DeviceArray, as_device_array, launch_stream, torch_on, use_stream
+
+_DTYPES = {"f8": _lib.F64, "f4": _lib.F32}
+#: Keywords of cunumpy kernel launches (src/mpifield/weighting.py:286-295): this
+#: backend sizes its own launches, so they change nothing here.
+_LAUNCH_KEYWORDS = frozenset({"shared_mem", "n_threads"})
 
 
-def _marker_rows(t: torch.Tensor, rows: int, name: str, dtype: torch.dtype) -> tuple[torch.Tensor, int]:
-    """``t`` as ``(rows, N)`` with unit column stride, and its row stride in elements."""
-    if t.dim() == 1:
-        t = t.reshape(1, -1)
-    if t.dim() != 2 or t.shape[0] != rows:
-        raise ValueError(f"{name} must be ({rows}, N), got {tuple(t.shape)}")
-    if t.dtype != dtype:
-        t = t.to(dtype)
-    if t.shape[1] > 1 and t.stride(1) != 1:
-        t = t.contiguous()
-    if t.shape[0] > 1 and t.stride(0) < t.shape[1]:
-        t = t.contiguous()
-    stride = t.stride(0) if t.shape[0] > 1 else t.shape[1]
-    return t, int(stride)
+def _dtype_code(a: DeviceArray, name: str) -> int:
+    if a.dtype not in _DTYPES:
+        raise TypeError(f"mpifield_b200 kernels take float64 or float32, {name} is {a.dtype}")
+    return _DTYPES[a.dtype]
+
+
+def _torch_dtype(code: str):
+    import torch
+
+    return {"f8": torch.float64, "f4": torch.float32}[code]
+
+
+def _copied(a: DeviceArray, shape: tuple[int, ...], dtype: str, stream: int) -> DeviceArray:
+    """A contiguous ``shape`` copy of ``a`` in ``dtype``, made on the launch stream."""
+    with torch_on(stream):
+        t = a.torch().reshape(shape).to(_torch_dtype(dtype)).contiguous()
+    return as_device_array(t)
+
+
+def _marker_rows(a: DeviceArray, rows: int, name: str, dtype: str, stream: int) -> tuple[DeviceArray, int]:
+    """``a`` as ``(rows, N)`` with unit column stride, and its row stride in elements; a
+    1-D array is one row. Copied only where the layout or element type needs it."""
+    if a.ndim == 1:
+        a = DeviceArray(a.ptr, (1, a.shape[0]), (a.shape[0], a.strides[0]), a.dtype, a.source, a.stream, a.device)
+    if a.ndim != 2 or a.shape[0] != rows:
+        raise ValueError(f"{name} must be ({rows}, N), got {a.shape}")
+    n = a.shape[1]
+    fits = a.dtype == dtype and (n <= 1 or a.strides[1] == 1) and (rows == 1 or a.strides[0] >= n)
+    if not fits:
+        a = _copied(a, (rows, n), dtype, stream)
+    return a, (a.strides[0] if rows > 1 else n)
 
 
 class _Output:
-    """A contiguous working copy of an output tensor, written back on exit if needed."""
+    """Where a call writes ``target``: the target itself when the C call takes its layout,
+    else a contiguous copy (filled from the target for an accumulating call) that
+    `finish` writes back, both on the launch stream."""
 
-    def __init__(self, target: torch.Tensor, dtype: torch.dtype, accumulate: bool):
-        self.target = target
-        self.direct = target.is_contiguous() and target.dtype == dtype
+    def __init__(self, target: DeviceArray, dtype: str, accumulate: bool, stream: int, rows: int | None = None):
+        self.target, self.stream = target, stream
+        if rows is None:
+            self.direct = target.is_contiguous() and target.dtype == dtype
+        else:
+            n = target.shape[-1]
+            self.direct = (target.dtype == dtype and target.ndim == 2 and (n <= 1 or target.strides[1] == 1)
+                           and (rows == 1 or target.strides[0] >= n))
         if self.direct:
             self.work = target
-        elif accumulate:
-            self.work = target.to(dtype).contiguous()
-        else:
-            self.work = torch.empty(target.shape, dtype=dtype, device=target.device)
+            return
+        import torch
+
+        with torch_on(stream):
+            if accumulate:
+                work = target.torch().to(_torch_dtype(dtype)).contiguous()
+                if work.data_ptr() == target.ptr:
+                    work = work.clone()
+            else:
+                work = torch.empty(target.shape, dtype=_torch_dtype(dtype), device=target.torch().device)
+        self.work = as_device_array(work)
+
+    @property
+    def row_stride(self) -> int:
+        return self.work.strides[0] if self.work.shape[0] > 1 else self.work.shape[-1]
 
     def finish(self) -> None:
         if not self.direct:
-            self.target.copy_(self.work)
+            with torch_on(self.stream):
+                self.target.torch().copy_(self.work.torch())
 
 
 def _extent(num, code, degree) -> tuple[int, ...]:
     return tuple(int(n) + (degree - 1 if int(c) == 2 else 0) for n, c in zip(num, code))
 
 
-def _field_shape(field: torch.Tensor, extent: tuple[int, ...], name: str) -> torch.Tensor:
-    """``field`` as ``extent + (ncomp,)``; a 1-D field or the linear 3D rows are reshaped."""
+def _field(a: DeviceArray, extent: tuple[int, ...], name: str) -> DeviceArray:
+    """``a`` as ``extent + (ncomp,)``: a field without the component axis is one
+    component, and the linear 3D kernels' rows ``(nx * ny * nz, ncomp)`` are the grid."""
     ndim = len(extent)
-    if field.dim() == ndim:
-        field = field.unsqueeze(-1)
-    elif ndim == 3 and field.dim() == 2 and field.shape[0] == extent[0] * extent[1] * extent[2]:
-        field = field.view(*extent, field.shape[1]) if field.is_contiguous() else field.reshape(*extent, field.shape[1])
-    if tuple(field.shape[:-1]) != extent or field.dim() != ndim + 1:
-        raise ValueError(f"{name} on this grid is {extent} + (ncomp,), got {tuple(field.shape)}")
-    return field
+    if a.ndim == ndim:
+        a = DeviceArray(a.ptr, a.shape + (1,), a.strides + (1,), a.dtype, a.source, a.stream, a.device)
+    elif ndim == 3 and a.ndim == 2 and a.shape[0] == extent[0] * extent[1] * extent[2]:
+        if not a.is_contiguous():
+            raise ValueError("the linear 3D kernels need a C-contiguous field")
+        a = a.reshaped((*extent, a.shape[1]))
+    if a.ndim != ndim + 1 or tuple(a.shape[:-1]) != extent:
+        raise ValueError(f"{name} on this grid is {extent} + (ncomp,), got {a.shape}")
+    return a
+
+
+def _arrays(**named) -> tuple[dict[str, DeviceArray], int]:
+    """Every named argument as a `DeviceArray` (None stays None), and the launch stream."""
+    arrays = {k: (None if v is None else as_device_array(v, k)) for k, v in named.items()}
+    present = [a for a in arrays.values() if a is not None]
+    devices = {a.device for a in present if a.device is not None}
+    if len(devices) > 1:
+        raise ValueError(f"arrays on different devices: {sorted(devices)}")
+    return arrays, launch_stream(*present)
+
+
+def _tile_args(order, ndim: int):
+    """The tile shape (ctypes array) and tile starts of a `sorting.TileOrder`, checked."""
+    starts = as_device_array(order.tile_start, "order.tile_start")
+    if starts.dtype != "i8" or not starts.is_contiguous():
+        raise ValueError("order.tile_start must be a contiguous int64 array on the markers' device")
+    if len(order.tile) != ndim or starts.size != order.num_tiles + 2:
+        raise ValueError(f"a tile order of {len(order.tile)} axes and {starts.size} starts for a {ndim}D grid")
+    return (C.c_int32 * ndim)(*(int(v) for v in order.tile)), starts.ptr
+
+
+def _degree(takes_degree: bool, fixed: int | None, args: tuple) -> tuple[int, tuple]:
+    if takes_degree:
+        *rest, degree = args
+        return int(degree), tuple(rest)
+    return int(fixed), args
+
+
+def _launch_options(kernel: str, launch: dict):
+    unknown = set(launch) - _LAUNCH_KEYWORDS - {"stream"}
+    if unknown:
+        raise TypeError(f"{kernel} got unexpected keyword arguments {sorted(unknown)}")
+    stream = launch.get("stream")
+    return use_stream(stream) if stream is not None else _NoStream()
+
+
+class _NoStream:
+    def __enter__(self):
+        return None
+
+    def __exit__(self, *exc):
+        return False
 
 
 @dataclass(frozen=True)
@@ -92,71 +183,56 @@ class NodeKernel:
     fixed_degree: int | None = None
     tuning: _lib.Tuning | None = None
 
-    def __call__(self, *args) -> None:
-        if self.takes_degree:
-            *args, degree = args
-            degree = int(degree)
-        else:
-            degree = int(self.fixed_degree)
-        if self.op == "gather":
-            positions, field, result, *geometry = args
-            gather(self.kind, degree, positions, field, result, geometry, self.tuning)
-        else:
-            positions, values, field, *geometry = args
-            scatter(self.kind, degree, positions, values, field, geometry, self.tuning)
+    def __call__(self, *args, **launch) -> None:
+        degree, args = _degree(self.takes_degree, self.fixed_degree, args)
+        with _launch_options(f"{self.op} kernel", launch):
+            if self.op == "gather":
+                positions, field, result, *geometry = args
+                gather(self.kind, degree, positions, field, result, geometry, self.tuning)
+            else:
+                positions, values, field, *geometry = args
+                scatter(self.kind, degree, positions, values, field, geometry, self.tuning)
 
 
-def _tile_args(order, ndim: int, device):
-    """The tile shape (ctypes array) and tile starts of a `sorting.TileOrder`, checked."""
-    starts = order.tile_start
-    if starts.device != device or starts.dtype != torch.int64 or not starts.is_contiguous():
-        raise ValueError("order.tile_start must be a contiguous int64 tensor on the markers' device")
-    if len(order.tile) != ndim or starts.numel() != order.num_tiles + 2:
-        raise ValueError(f"a tile order of {len(order.tile)} axes and {starts.numel()} starts for a {ndim}D grid")
-    return (C.c_int32 * ndim)(*(int(v) for v in order.tile)), starts.data_ptr()
-
-
-def gather(kind: int, degree: int, positions: torch.Tensor, field: torch.Tensor, result: torch.Tensor,
-           geometry, tuning: _lib.Tuning | None = None, order=None) -> None:
+def gather(kind: int, degree: int, positions, field, result, geometry, tuning: _lib.Tuning | None = None,
+           order=None) -> None:
     """result(c, i) = sum_k W_k(x_i) field(k, c), overwriting ``result`` (ncomp, N).
 
     ``order``: the `sorting.TileOrder` whose rank order the markers are in, for
     ``mpf_gather_tiles`` (the same result, whatever the markers' order).
     """
     lower, cell, num, code, ndim = _lib.geometry_arrays(geometry)
-    device = _lib.require_cuda(positions, field, result)
-    dtype = field.dtype
-    dcode = _lib.dtype_code(dtype)
-    field = _field_shape(field, _extent(num, code, degree), "field")
-    if not field.is_contiguous():
-        field = field.contiguous()
-    ncomp = field.shape[-1]
-    pos, ps = _marker_rows(positions, ndim, "positions", dtype)
+    a, stream = _arrays(positions=positions, field=field, result=result)
+    dtype = a["field"].dtype
+    dcode = _dtype_code(a["field"], "field")
+    f = _field(a["field"], _extent(num, code, degree), "field")
+    if not f.is_contiguous():
+        f = _copied(f, f.shape, dtype, stream)
+    ncomp = f.shape[-1]
+    pos, ps = _marker_rows(a["positions"], ndim, "positions", dtype, stream)
     n = pos.shape[1]
-    if result.dim() == 1:
-        result = result.view(1, -1)
-    if tuple(result.shape) != (ncomp, n):
-        raise ValueError(f"result must be ({ncomp}, {n}), got {tuple(result.shape)}")
-    rows_ok = result.dtype == dtype and (n <= 1 or result.stride(1) == 1) and (ncomp == 1 or result.stride(0) >= n)
-    out = result if rows_ok else torch.empty((ncomp, n), dtype=dtype, device=device)
-    rs = out.stride(0) if ncomp > 1 else n
+    res = a["result"]
+    if res.ndim == 1:
+        res = DeviceArray(res.ptr, (1, res.shape[0]), (res.shape[0], res.strides[0]), res.dtype, res.source,
+                          res.stream, res.device)
+    if res.shape != (ncomp, n):
+        raise ValueError(f"result must be ({ncomp}, {n}), got {res.shape}")
+    out = _Output(res, dtype, accumulate=False, stream=stream, rows=ncomp)
     tune = C.byref(tuning) if tuning is not None else None
+    lib = _lib.library()
     if order is None:
-        status = _lib.library().mpf_gather(
-            kind, degree, ndim, pos.data_ptr(), ps, n, field.data_ptr(), ncomp, out.data_ptr(), rs,
-            lower, cell, num, code, dcode, tune, _lib.stream_of(device))
+        status = lib.mpf_gather(kind, degree, ndim, pos.ptr, ps, n, f.ptr, ncomp, out.work.ptr, out.row_stride,
+                                lower, cell, num, code, dcode, tune, stream)
     else:
-        tile, starts = _tile_args(order, ndim, device)
-        status = _lib.library().mpf_gather_tiles(
-            kind, degree, ndim, pos.data_ptr(), ps, n, field.data_ptr(), ncomp, out.data_ptr(), rs,
-            lower, cell, num, code, tile, starts, dcode, tune, _lib.stream_of(device))
+        tile, starts = _tile_args(order, ndim)
+        status = lib.mpf_gather_tiles(kind, degree, ndim, pos.ptr, ps, n, f.ptr, ncomp, out.work.ptr,
+                                      out.row_stride, lower, cell, num, code, tile, starts, dcode, tune, stream)
     _lib.check(status, "gather")
-    if out is not result:
-        result.copy_(out)
+    out.finish()
 
 
-def scatter(kind: int, degree: int, positions: torch.Tensor, values: torch.Tensor, field: torch.Tensor,
-            geometry, tuning: _lib.Tuning | None = None, order=None) -> None:
+def scatter(kind: int, degree: int, positions, values, field, geometry, tuning: _lib.Tuning | None = None,
+            order=None) -> None:
     """field(k, c) += sum_i W_k(x_i) values(c, i); dead markers (all values zero) skipped.
 
     ``order``: the `sorting.TileOrder` whose rank order the markers are in (positions and
@@ -164,32 +240,32 @@ def scatter(kind: int, degree: int, positions: torch.Tensor, values: torch.Tenso
     up to the order of the floating-point adds, whatever the markers' order.
     """
     lower, cell, num, code, ndim = _lib.geometry_arrays(geometry)
-    device = _lib.require_cuda(positions, values, field)
-    dtype = field.dtype
-    dcode = _lib.dtype_code(dtype)
-    shaped = _field_shape(field, _extent(num, code, degree), "field")
-    ncomp = shaped.shape[-1]
-    pos, ps = _marker_rows(positions, ndim, "positions", dtype)
-    vals, vs = _marker_rows(values, ncomp, "values", dtype)
+    a, stream = _arrays(positions=positions, values=values, field=field)
+    dtype = a["field"].dtype
+    dcode = _dtype_code(a["field"], "field")
+    f = _field(a["field"], _extent(num, code, degree), "field")
+    ncomp = f.shape[-1]
+    pos, ps = _marker_rows(a["positions"], ndim, "positions", dtype, stream)
+    vals, vs = _marker_rows(a["values"], ncomp, "values", dtype, stream)
     if vals.shape[1] != pos.shape[1]:
         raise ValueError(f"{pos.shape[1]} positions and {vals.shape[1]} values")
-    out = _Output(shaped, dtype, accumulate=True)
+    out = _Output(f, dtype, accumulate=True, stream=stream)
     tune = C.byref(tuning) if tuning is not None else None
+    lib = _lib.library()
+    n = pos.shape[1]
     if order is None:
-        status = _lib.library().mpf_scatter(
-            kind, degree, ndim, pos.data_ptr(), ps, vals.data_ptr(), vs, pos.shape[1], out.work.data_ptr(),
-            ncomp, lower, cell, num, code, dcode, tune, _lib.stream_of(device))
+        status = lib.mpf_scatter(kind, degree, ndim, pos.ptr, ps, vals.ptr, vs, n, out.work.ptr, ncomp, lower, cell,
+                                 num, code, dcode, tune, stream)
     else:
-        tile, starts = _tile_args(order, ndim, device)
-        status = _lib.library().mpf_scatter_tiles(
-            kind, degree, ndim, pos.data_ptr(), ps, vals.data_ptr(), vs, pos.shape[1], out.work.data_ptr(),
-            ncomp, lower, cell, num, code, tile, starts, dcode, tune, _lib.stream_of(device))
+        tile, starts = _tile_args(order, ndim)
+        status = lib.mpf_scatter_tiles(kind, degree, ndim, pos.ptr, ps, vals.ptr, vs, n, out.work.ptr, ncomp, lower,
+                                       cell, num, code, tile, starts, dcode, tune, stream)
     _lib.check(status, "scatter")
     out.finish()
 
 
-def scatter_deterministic(kind: int, degree: int, positions: torch.Tensor, values: torch.Tensor,
-                          field: torch.Tensor, geometry, workspace: torch.Tensor | None = None, order=None) -> None:
+def scatter_deterministic(kind: int, degree: int, positions, values, field, geometry, workspace=None,
+                          order=None) -> None:
     """field(k, c) += sum_i W_k(x_i) values(c, i), the same bits for every run and marker
     order (``mpf_scatter_deterministic``: fixed-point integer sums); float64 only.
 
@@ -197,129 +273,141 @@ def scatter_deterministic(kind: int, degree: int, positions: torch.Tensor, value
     ``mpf_scatter_deterministic_tiles`` (the same bits).
     """
     lower, cell, num, code, ndim = _lib.geometry_arrays(geometry)
-    device = _lib.require_cuda(positions, values, field)
-    if field.dtype != torch.float64:
+    a, stream = _arrays(positions=positions, values=values, field=field, workspace=workspace)
+    if a["field"].dtype != "f8":
         raise TypeError("the deterministic scatter is float64 only")
-    shaped = _field_shape(field, _extent(num, code, degree), "field")
-    ncomp = shaped.shape[-1]
-    pos, ps = _marker_rows(positions, ndim, "positions", torch.float64)
-    vals, vs = _marker_rows(values, ncomp, "values", torch.float64)
+    f = _field(a["field"], _extent(num, code, degree), "field")
+    ncomp = f.shape[-1]
+    pos, ps = _marker_rows(a["positions"], ndim, "positions", "f8", stream)
+    vals, vs = _marker_rows(a["values"], ncomp, "values", "f8", stream)
     if vals.shape[1] != pos.shape[1]:
         raise ValueError(f"{pos.shape[1]} positions and {vals.shape[1]} values")
     size = C.c_size_t(0)
-    _lib.check(_lib.library().mpf_scatter_deterministic_workspace_bytes(shaped.numel(), C.byref(size)),
+    lib = _lib.library()
+    _lib.check(lib.mpf_scatter_deterministic_workspace_bytes(f.size, C.byref(size)),
                "scatter_deterministic_workspace_bytes")
-    if workspace is None or workspace.numel() * workspace.element_size() < size.value:
-        workspace = torch.empty(size.value, dtype=torch.uint8, device=device)
-    out = _Output(shaped, torch.float64, accumulate=True)
-    wbytes = workspace.numel() * workspace.element_size()
+    ws = a["workspace"]
+    if ws is None or ws.size * ws.itemsize < size.value:
+        import torch
+
+        with torch_on(stream):
+            ws = as_device_array(torch.empty(size.value, dtype=torch.uint8, device=f.torch().device))
+    out = _Output(f, "f8", accumulate=True, stream=stream)
+    wbytes = ws.size * ws.itemsize
+    n = pos.shape[1]
     if order is None:
-        status = _lib.library().mpf_scatter_deterministic(
-            kind, degree, ndim, pos.data_ptr(), ps, vals.data_ptr(), vs, pos.shape[1], out.work.data_ptr(), ncomp,
-            lower, cell, num, code, workspace.data_ptr(), wbytes, _lib.stream_of(device))
+        status = lib.mpf_scatter_deterministic(kind, degree, ndim, pos.ptr, ps, vals.ptr, vs, n, out.work.ptr, ncomp,
+                                               lower, cell, num, code, ws.ptr, wbytes, stream)
     else:
-        tile, starts = _tile_args(order, ndim, device)
-        status = _lib.library().mpf_scatter_deterministic_tiles(
-            kind, degree, ndim, pos.data_ptr(), ps, vals.data_ptr(), vs, pos.shape[1], out.work.data_ptr(), ncomp,
-            lower, cell, num, code, tile, starts, workspace.data_ptr(), wbytes, _lib.stream_of(device))
+        tile, starts = _tile_args(order, ndim)
+        status = lib.mpf_scatter_deterministic_tiles(kind, degree, ndim, pos.ptr, ps, vals.ptr, vs, n, out.work.ptr,
+                                                     ncomp, lower, cell, num, code, tile, starts, ws.ptr, wbytes,
+                                                     stream)
     _lib.check(status, "scatter_deterministic")
     out.finish()
 
 
-def gather_grad(kind: int, degree: int, positions: torch.Tensor, field: torch.Tensor,
-                cotangent: torch.Tensor, geometry) -> torch.Tensor:
-    """``(ndim, N)``: d/dx_d of sum_c cotangent(c, i) gather_c(x_i), the position gradient."""
+def gather_grad(kind: int, degree: int, positions, field, cotangent, geometry):
+    """``(ndim, N)`` torch tensor: d/dx_d of sum_c cotangent(c, i) gather_c(x_i), the position gradient."""
+    import torch
+
     lower, cell, num, code, ndim = _lib.geometry_arrays(geometry)
-    device = _lib.require_cuda(positions, field, cotangent)
-    dtype = field.dtype
-    field = _field_shape(field, _extent(num, code, degree), "field").contiguous()
-    ncomp = field.shape[-1]
-    pos, ps = _marker_rows(positions, ndim, "positions", dtype)
-    cot, cs = _marker_rows(cotangent, ncomp, "cotangent", dtype)
+    a, stream = _arrays(positions=positions, field=field, cotangent=cotangent)
+    dtype = a["field"].dtype
+    f = _field(a["field"], _extent(num, code, degree), "field")
+    if not f.is_contiguous():
+        f = _copied(f, f.shape, dtype, stream)
+    ncomp = f.shape[-1]
+    pos, ps = _marker_rows(a["positions"], ndim, "positions", dtype, stream)
+    cot, cs = _marker_rows(a["cotangent"], ncomp, "cotangent", dtype, stream)
     n = pos.shape[1]
-    grad = torch.empty((ndim, n), dtype=dtype, device=device)
+    with torch_on(stream):
+        grad = torch.empty((ndim, n), dtype=_torch_dtype(dtype), device=f.torch().device)
     status = _lib.library().mpf_gather_grad(
-        kind, degree, ndim, pos.data_ptr(), ps, n, field.data_ptr(), ncomp, cot.data_ptr(), cs,
-        grad.data_ptr(), n, lower, cell, num, code, _lib.dtype_code(dtype), _lib.stream_of(device))
+        kind, degree, ndim, pos.ptr, ps, n, f.ptr, ncomp, cot.ptr, cs, grad.data_ptr(), n, lower, cell, num, code,
+        _dtype_code(f, "field"), stream)
     _lib.check(status, "gather_grad")
     return grad
 
 
 @dataclass(frozen=True)
 class PathKernel:
-    """A path deposit: WHITNEY (kind LINEAR) or the spline edges (kind SPLINE + degree)."""
+    """A path deposit: WHITNEY (kind LINEAR, degree 1) or the spline edges (kind SPLINE),
+    whose degree is the last argument (``takes_degree``) or ``fixed_degree``."""
 
     kind: int
     ndim: int
     takes_degree: bool
+    fixed_degree: int = 1
 
-    def __call__(self, *args) -> None:
-        if self.takes_degree:
-            *args, degree = args
-            degree = int(degree)
-        else:
-            degree = 1
+    def __call__(self, *args, **launch) -> None:
+        degree, args = _degree(self.takes_degree, self.fixed_degree, args)
         start, end, charges, edges, *geometry = args
-        deposit_paths(self.kind, degree, start, end, charges, edges, geometry)
+        with _launch_options("deposit_paths kernel", launch):
+            deposit_paths(self.kind, degree, start, end, charges, edges, geometry)
 
 
 @dataclass(frozen=True)
 class EdgeGatherKernel:
+    """An edge gather: the Whitney edge functions (kind LINEAR) or the spline edges, with
+    the degree as for `PathKernel`."""
+
     kind: int
     ndim: int
     takes_degree: bool
+    fixed_degree: int = 1
 
-    def __call__(self, *args) -> None:
-        if self.takes_degree:
-            *args, degree = args
-            degree = int(degree)
-        else:
-            degree = 1
+    def __call__(self, *args, **launch) -> None:
+        degree, args = _degree(self.takes_degree, self.fixed_degree, args)
         positions, edges, result, *geometry = args
-        gather_edges(self.kind, degree, positions, edges, result, geometry)
+        with _launch_options("gather_edges kernel", launch):
+            gather_edges(self.kind, degree, positions, edges, result, geometry)
 
 
-def deposit_paths(kind: int, degree: int, start: torch.Tensor, end: torch.Tensor, charges: torch.Tensor,
-                  edges: torch.Tensor, geometry, tuning: _lib.Tuning | None = None) -> None:
+def _edge_field(a: DeviceArray, num, code, degree, ndim) -> None:
+    extent = _extent(num, code, degree)
+    if a.shape != (*extent, ndim):
+        raise ValueError(f"an edge field on this grid is {(*extent, ndim)}, got {a.shape}")
+
+
+def deposit_paths(kind: int, degree: int, start, end, charges, edges, geometry,
+                  tuning: _lib.Tuning | None = None) -> None:
     """edges += the current of ``charges`` moving from ``start`` to ``end`` (ndim, N)."""
     lower, cell, num, code, ndim = _lib.geometry_arrays(geometry)
-    device = _lib.require_cuda(start, end, charges, edges)
-    dtype = edges.dtype
-    s, ss = _marker_rows(start, ndim, "start", dtype)
-    e, es = _marker_rows(end, ndim, "end", dtype)
-    q = charges.reshape(-1).to(dtype).contiguous()
-    if s.shape != e.shape or s.shape[1] != q.shape[0]:
-        raise ValueError(f"paths from {tuple(s.shape)} to {tuple(e.shape)} for {q.shape[0]} charges")
-    extent = _extent(num, code, degree)
-    if tuple(edges.shape) != (*extent, ndim):
-        raise ValueError(f"an edge field on this grid is {(*extent, ndim)}, got {tuple(edges.shape)}")
-    out = _Output(edges, dtype, accumulate=True)
+    a, stream = _arrays(start=start, end=end, charges=charges, edges=edges)
+    dtype = a["edges"].dtype
+    s, ss = _marker_rows(a["start"], ndim, "start", dtype, stream)
+    e, es = _marker_rows(a["end"], ndim, "end", dtype, stream)
+    q = a["charges"]
+    if q.ndim > 1:  # (1, N) or any array of N charges
+        q = q.reshaped((q.size,)) if q.is_contiguous() else _copied(q, (q.size,), dtype, stream)
+    q, _ = _marker_rows(q, 1, "charges", dtype, stream)
+    if s.shape != e.shape or s.shape[1] != q.shape[1]:
+        raise ValueError(f"paths from {s.shape} to {e.shape} for {q.shape[1]} charges")
+    _edge_field(a["edges"], num, code, degree, ndim)
+    out = _Output(a["edges"], dtype, accumulate=True, stream=stream)
     status = _lib.library().mpf_deposit_paths(
-        kind, degree, ndim, s.data_ptr(), ss, e.data_ptr(), es, q.data_ptr(), q.shape[0],
-        out.work.data_ptr(), lower, cell, num, code, _lib.dtype_code(dtype),
-        C.byref(tuning) if tuning is not None else None, _lib.stream_of(device))
+        kind, degree, ndim, s.ptr, ss, e.ptr, es, q.ptr, q.shape[1], out.work.ptr, lower, cell, num, code,
+        _dtype_code(a["edges"], "edges"), C.byref(tuning) if tuning is not None else None, stream)
     _lib.check(status, "deposit_paths")
     out.finish()
 
 
-def gather_edges(kind: int, degree: int, positions: torch.Tensor, edges: torch.Tensor, result: torch.Tensor,
-                 geometry) -> None:
+def gather_edges(kind: int, degree: int, positions, edges, result, geometry) -> None:
     """result(a, i) = the field of the edge field along axis a at marker i."""
     lower, cell, num, code, ndim = _lib.geometry_arrays(geometry)
-    device = _lib.require_cuda(positions, edges, result)
-    dtype = edges.dtype
-    pos, ps = _marker_rows(positions, ndim, "positions", dtype)
+    a, stream = _arrays(positions=positions, edges=edges, result=result)
+    dtype = a["edges"].dtype
+    pos, ps = _marker_rows(a["positions"], ndim, "positions", dtype, stream)
     n = pos.shape[1]
-    extent = _extent(num, code, degree)
-    if tuple(edges.shape) != (*extent, ndim):
-        raise ValueError(f"an edge field on this grid is {(*extent, ndim)}, got {tuple(edges.shape)}")
-    edges = edges.contiguous()
-    out = _Output(result, dtype, accumulate=False)
-    if tuple(out.work.shape) != (ndim, n):
-        raise ValueError(f"result must be ({ndim}, {n}), got {tuple(result.shape)}")
+    _edge_field(a["edges"], num, code, degree, ndim)
+    ed = a["edges"] if a["edges"].is_contiguous() else _copied(a["edges"], a["edges"].shape, dtype, stream)
+    if a["result"].shape != (ndim, n):
+        raise ValueError(f"result must be ({ndim}, {n}), got {a['result'].shape}")
+    out = _Output(a["result"], dtype, accumulate=False, stream=stream, rows=ndim)
     status = _lib.library().mpf_gather_edges(
-        kind, degree, ndim, pos.data_ptr(), ps, n, edges.data_ptr(), out.work.data_ptr(), out.work.stride(0),
-        lower, cell, num, code, _lib.dtype_code(dtype), _lib.stream_of(device))
+        kind, degree, ndim, pos.ptr, ps, n, ed.ptr, out.work.ptr, out.row_stride, lower, cell, num, code,
+        _dtype_code(ed, "edges"), stream)
     _lib.check(status, "gather_edges")
     out.finish()
 

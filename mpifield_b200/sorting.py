@@ -19,6 +19,7 @@ from dataclasses import dataclass
 import torch
 
 from mpifield_b200 import _lib
+from mpifield_b200._arrays import as_device_array, launch_stream, torch_on
 from mpifield_b200.kernels import _marker_rows
 
 
@@ -57,6 +58,11 @@ def sort_workspace_bytes(n: int, ntiles: int) -> int:
     return max(int(size.value), 256)
 
 
+def _code_of(dtype: torch.dtype) -> str:
+    _lib.dtype_code(dtype)  # float64 or float32 only
+    return "f8" if dtype == torch.float64 else "f4"
+
+
 def _empty(shape, dtype, device):
     return torch.empty(shape, dtype=dtype, device=device)
 
@@ -72,26 +78,31 @@ def sort_by_tile(positions: torch.Tensor, weighting, geometry, tile, values: tor
     """
     kind, degree = _kind_of(weighting)
     lower, cell, num, code, ndim = _lib.geometry_arrays(geometry)
-    device = _lib.require_cuda(positions)
-    dtype = positions.dtype
-    pos, ps = _marker_rows(positions, ndim, "positions", dtype)
+    p = as_device_array(positions, "positions")
+    v = None if values is None else as_device_array(values, "values")
+    stream = launch_stream(*(a for a in (p, v) if a is not None))
+    if p.dtype not in ("f8", "f4"):
+        raise TypeError(f"positions must be float64 or float32, got {p.dtype}")
+    pos, ps = _marker_rows(p, ndim, "positions", p.dtype, stream)
     n = pos.shape[1]
     ntiles = num_tiles((kind, degree), geometry, tile)
     t = (C.c_int32 * ndim)(*(int(v) for v in tile))
+    device = pos.torch().device
     new = alloc or (lambda shape, dt: _empty(shape, dt, device))
-    workspace = new((sort_workspace_bytes(n, ntiles),), torch.uint8)
-    keys = new((n,), torch.int32)
-    order = new((n,), torch.int32)
-    tile_start = new((ntiles + 2,), torch.int64)
-    if values is not None:
-        vals, vs = _marker_rows(values, values.shape[0] if values.dim() == 2 else 1, "values", dtype)
-        vptr, ncomp = vals.data_ptr(), vals.shape[0]
+    with torch_on(stream):
+        workspace = new((sort_workspace_bytes(n, ntiles),), torch.uint8)
+        keys = new((n,), torch.int32)
+        order = new((n,), torch.int32)
+        tile_start = new((ntiles + 2,), torch.int64)
+    if v is not None:
+        vals, vs = _marker_rows(v, v.shape[0] if v.ndim == 2 else 1, "values", p.dtype, stream)
+        vptr, ncomp = vals.ptr, vals.shape[0]
     else:
         vptr, vs, ncomp = None, 0, 0
     status = _lib.library().mpf_sort_by_tile(
-        kind, degree, ndim, pos.data_ptr(), ps, vptr, vs, ncomp, n, lower, cell, num, code, t, int(bool(within)),
+        kind, degree, ndim, pos.ptr, ps, vptr, vs, ncomp, n, lower, cell, num, code, t, int(bool(within)),
         keys.data_ptr(), order.data_ptr(), tile_start.data_ptr(), workspace.data_ptr(), workspace.numel(),
-        _lib.dtype_code(dtype), _lib.stream_of(device))
+        _lib.F64 if p.dtype == "f8" else _lib.F32, stream)
     _lib.check(status, "sort_by_tile")
     return TileOrder(keys, order, tile_start, ntiles, tuple(int(v) for v in tile))
 
@@ -102,14 +113,15 @@ def permute(array: torch.Tensor, order: torch.Tensor, out: torch.Tensor | None =
     device = _lib.require_cuda(array, order)
     squeeze = array.dim() == 1
     rows = 1 if squeeze else array.shape[0]
-    src, ss = _marker_rows(array, rows, "array", array.dtype)
+    stream = _lib.stream_of(device)
+    src, ss = _marker_rows(as_device_array(array), rows, "array", _code_of(array.dtype), stream)
     n = src.shape[1]
     dst = torch.empty((rows, n), dtype=array.dtype, device=device) if out is None else out.view(rows, n)
     if not dst.is_contiguous() or dst.dtype != array.dtype:
         raise ValueError(f"out must be a contiguous ({rows}, {n}) {array.dtype} tensor")
     order = order.to(torch.int32).contiguous()
-    status = _lib.library().mpf_permute_rows(dst.data_ptr(), n, src.data_ptr(), ss, rows, order.data_ptr(), n,
-                                            _lib.dtype_code(array.dtype), _lib.stream_of(device))
+    status = _lib.library().mpf_permute_rows(dst.data_ptr(), n, src.ptr, ss, rows, order.data_ptr(), n,
+                                            _lib.dtype_code(array.dtype), stream)
     _lib.check(status, "permute_rows")
     return dst[0] if squeeze else dst
 
@@ -119,7 +131,8 @@ def unpermute(array: torch.Tensor, order: torch.Tensor, out: torch.Tensor | None
     device = _lib.require_cuda(array, order)
     squeeze = array.dim() == 1
     rows = 1 if squeeze else array.shape[0]
-    src, ss = _marker_rows(array, rows, "array", array.dtype)
+    stream = _lib.stream_of(device)
+    src, ss = _marker_rows(as_device_array(array), rows, "array", _code_of(array.dtype), stream)
     n = src.shape[1]
     dst = out if out is not None else torch.empty((rows, n), dtype=array.dtype, device=device)
     if dst.dim() == 1:
@@ -127,7 +140,7 @@ def unpermute(array: torch.Tensor, order: torch.Tensor, out: torch.Tensor | None
     if not dst.is_contiguous() or tuple(dst.shape) != (rows, n):
         raise ValueError(f"out must be a contiguous ({rows}, {n}) tensor")
     order = order.to(torch.int32).contiguous()
-    status = _lib.library().mpf_unpermute_rows(dst.data_ptr(), n, src.data_ptr(), ss, rows, order.data_ptr(), n,
-                                              _lib.dtype_code(array.dtype), _lib.stream_of(device))
+    status = _lib.library().mpf_unpermute_rows(dst.data_ptr(), n, src.ptr, ss, rows, order.data_ptr(), n,
+                                              _lib.dtype_code(array.dtype), stream)
     _lib.check(status, "unpermute_rows")
     return dst[0] if squeeze else dst

@@ -1,14 +1,18 @@
-"""The node and edge weighting of each B-spline degree, paired (src/mpifield/splines.py:100-272).
+"""The B-spline families: the node and edge weightings of one degree, paired.
 
-Faces and cells (2-forms, top forms) are not part of this backend: `Splines` here holds
-``nodes`` and ``edges`` only.
+mpifield's ``Splines`` (src/mpifield/splines.py:100-272) names, for a degree, the
+weighting of every form: ``nodes`` (0-forms), ``edges`` (1-forms), ``faces`` (2-forms,
+3D) and ``cells`` (top forms). This backend covers the node and edge weightings of
+degrees 1-3 with its own kernels; `faces` and `cells` stay None here. `SPLINES` holds
+the built-in families; `CLAMPED_SPLINES` those whose weightings all take clamped axes
+(every one on the spline kernels), and `splines` picks one.
 """
 
 from __future__ import annotations
 
 from dataclasses import dataclass
 
-from mpifield_b200.edges import CUBIC_EDGES, QUADRATIC_EDGES, WHITNEY, EdgeWeighting, _spline_edges
+from mpifield_b200.edges import CUBIC_EDGES, QUADRATIC_EDGES, WHITNEY, EdgeWeighting, spline_edges
 from mpifield_b200.weighting import CUBIC, LINEAR, QUADRATIC, Weighting, spline_weighting
 
 __all__ = ["CLAMPED_SPLINES", "SPLINES", "Splines", "splines"]
@@ -16,72 +20,79 @@ __all__ = ["CLAMPED_SPLINES", "SPLINES", "Splines", "splines"]
 
 @dataclass(frozen=True, eq=False, repr=False)
 class Splines:
-    """The node weighting of B-spline degree ``degree`` and the edge weighting that matches it."""
+    """The weightings of B-spline degree ``degree``, one per form; ``edges``, ``faces``
+    and ``cells`` may be None. With ``clamped`` every weighting must take clamped axes."""
 
     degree: int
     nodes: Weighting
     edges: EdgeWeighting | None = None
+    faces: Weighting | None = None
+    cells: Weighting | None = None
     clamped: bool = False
 
     def __post_init__(self) -> None:
-        if self.nodes.degree != self.degree:
-            raise ValueError(
-                f"the node weighting {self.nodes.name!r} has degree {self.nodes.degree}, not {self.degree}")
-        if self.edges is not None and self.edges.degree != self.degree:
-            raise ValueError(
-                f"the edge weighting {self.edges.name!r} has degree {self.edges.degree}, not {self.degree}")
+        for role, weighting in (("node", self.nodes), ("edge", self.edges)):
+            if weighting is not None and weighting.degree != self.degree:
+                raise ValueError(
+                    f"the {role} weighting {weighting.name!r} has degree {weighting.degree}, not {self.degree}")
         if self.clamped:
-            for weighting in (self.nodes, self.edges):
-                if weighting is not None and not weighting.clamps:
-                    raise ValueError(f"the {weighting.name} weighting does not take clamped axes")
+            refusing = [w for w in self.forms() if not w.clamps]
+            if refusing:
+                raise ValueError(f"the {refusing[0].name} weighting does not take clamped axes")
+
+    def forms(self) -> tuple:
+        """The weightings present, nodes first."""
+        return tuple(w for w in (self.nodes, self.edges, self.faces, self.cells) if w is not None)
 
     @property
     def halo(self) -> int:
-        edges = 0 if self.edges is None else self.edges.halo
-        return max(self.nodes.halo, edges)
+        """The halo a split field needs for the node and edge weightings together."""
+        return max(w.halo for w in (self.nodes, self.edges) if w is not None)
 
     def require_edges(self) -> EdgeWeighting:
-        if self.edges is None:
-            have = ", ".join(str(s.degree) for s in SPLINES.values() if s.edges)
-            raise ValueError(f"degree {self.degree} has no edge weighting yet (degrees with one: {have})")
-        return self.edges
+        """The edge weighting; ValueError for a family without one."""
+        if self.edges is not None:
+            return self.edges
+        have = ", ".join(str(d) for d, s in SPLINES.items() if s.edges is not None)
+        raise ValueError(f"degree {self.degree} has no edge weighting yet (degrees with one: {have})")
 
     def __repr__(self) -> str:
-        edges = None if self.edges is None else self.edges.name
-        clamped = ", clamped=True" if self.clamped else ""
-        return f"Splines(degree={self.degree}, nodes={self.nodes.name!r}, edges={edges!r}{clamped})"
+        names = ", ".join(f"{label}={w.name!r}" for label, w in
+                          (("nodes", self.nodes), ("edges", self.edges), ("faces", self.faces),
+                           ("cells", self.cells)) if w is not None)
+        return f"Splines(degree {self.degree}: {names}{', clamped' if self.clamped else ''})"
 
 
-def _clamping_nodes(name: str, degree: int) -> Weighting:
-    w = spline_weighting(degree, name)
-    return Weighting(name, scatter=w.scatter, gather=w.gather, halo=2 if degree > 1 else 1,
-                     degree=degree, clamps=True)
+def _family(degree: int, clamped: bool) -> Splines:
+    if not clamped:
+        nodes = {1: LINEAR, 2: QUADRATIC, 3: CUBIC}[degree]
+        edges = {1: WHITNEY, 2: QUADRATIC_EDGES, 3: CUBIC_EDGES}[degree]
+        return Splines(degree, nodes, edges)
+    # on clamped axes every weighting runs on the spline kernels (degree 3 already does)
+    name = {1: "linear", 2: "quadratic", 3: "cubic"}[degree]
+    nodes = CUBIC if degree == 3 else spline_weighting(degree, name)
+    nodes = Weighting(nodes.name, nodes.scatter, nodes.gather, halo=2 if degree > 1 else 1, degree=degree,
+                      clamps=True)
+    edges = {1: spline_edges("linear", 1), 2: QUADRATIC_EDGES, 3: CUBIC_EDGES}[degree]
+    return Splines(degree, nodes, edges, clamped=True)
 
 
-#: The built-in shapes, by degree.
-SPLINES: dict[int, Splines] = {
-    1: Splines(1, LINEAR, WHITNEY),
-    2: Splines(2, QUADRATIC, QUADRATIC_EDGES),
-    3: Splines(3, CUBIC, CUBIC_EDGES),
-}
-
-#: The built-in shapes whose weightings all take clamped axes (the spline kernels).
-CLAMPED_SPLINES: dict[int, Splines] = {
-    1: Splines(1, _clamping_nodes("linear", 1), _spline_edges("linear", 1), clamped=True),
-    2: Splines(2, _clamping_nodes("quadratic", 2), QUADRATIC_EDGES, clamped=True),
-    3: Splines(3, CUBIC, CUBIC_EDGES, clamped=True),
-}
+#: The built-in families, by degree.
+SPLINES: dict[int, Splines] = {d: _family(d, False) for d in (1, 2, 3)}
+#: The built-in families whose weightings all take clamped axes, by degree.
+CLAMPED_SPLINES: dict[int, Splines] = {d: _family(d, True) for d in (1, 2, 3)}
 
 
 def splines(degree: int | Splines, clamped: bool = False) -> Splines:
-    """The built-in `Splines` of a degree (a `Splines` is returned as is)."""
+    """The built-in `Splines` of a degree (from `CLAMPED_SPLINES` with ``clamped``); a
+    `Splines` is returned as it is, if it takes clamped axes where asked to."""
     if isinstance(degree, Splines):
         if clamped and not degree.clamped:
             raise ValueError(f"{degree!r} does not take clamped axes")
         return degree
     if isinstance(degree, bool) or int(degree) != degree:
         raise ValueError(f"a spline degree is an integer, got {degree!r}")
-    try:
-        return (CLAMPED_SPLINES if clamped else SPLINES)[int(degree)]
-    except KeyError:
-        raise ValueError(f"no built-in splines of degree {degree}; have {tuple(SPLINES)}") from None
+    table = CLAMPED_SPLINES if clamped else SPLINES
+    if int(degree) not in table:
+        raise ValueError(f"no built-in splines of degree {degree}; have {tuple(SPLINES)}")
+    return table[int(degree)]

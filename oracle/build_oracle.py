@@ -35,7 +35,8 @@ ORACLE_SO = HERE / "libmpf_oracle.so"
 REF_HOST_SO = REF_OUT / "libref_host.so"
 REF_C_SO = REF_OUT / "libref_c.so"
 REF_CUDA_SO = REF_OUT / "libref_cuda.so"
-REFERENCE_SRC = Path(os.environ.get("MPF_REFERENCE_SRC", "/root/reference/src"))
+# the mpifield sources: MPF_REFERENCE_SRC, else the reference/src folder beside this repository
+REFERENCE_SRC = Path(os.environ.get("MPF_REFERENCE_SRC", Path(__file__).resolve().parents[2] / "reference" / "src"))
 KERNELS = REFERENCE_SRC / "mpifield" / "kernels"
 
 #: The reference kernels compiled into the _ref libraries: the hot path and the edge gathers.

@@ -1,7 +1,7 @@
 """Generate the golden fixtures of tests/golden from the reference's own NumPy kernels.
 
-Run in a container that holds the mpifield source tree (default ``/root/reference/src``,
-or ``MPF_REFERENCE_SRC``)::
+Run where the mpifield source tree is at hand (``MPF_REFERENCE_SRC``, by default the
+``reference/src`` folder beside this repository)::
 
     python tests/golden/make_golden.py
 
@@ -33,7 +33,7 @@ from pathlib import Path
 import numpy as np
 
 OUT = Path(__file__).resolve().parent
-SRC = Path(os.environ.get("MPF_REFERENCE_SRC", "/root/reference/src"))
+SRC = Path(os.environ.get("MPF_REFERENCE_SRC", Path(__file__).resolve().parents[3] / "reference" / "src"))
 
 
 def _load_reference() -> None:

@@ -157,8 +157,15 @@ def test_weighting_checks_and_reprs():
         mf.Weighting("bad", scatter={}, gather={}, degree=-1)
     assert (mf.LINEAR.halo, mf.QUADRATIC.halo, mf.CUBIC.halo) == (1, 2, 2)
     assert (mf.LINEAR.degree, mf.QUADRATIC.degree, mf.CUBIC.degree) == (1, 2, 3)
-    assert repr(mf.CUBIC) == "Weighting('cubic', ndim=(1, 2, 3), halo=2, degree=3)"
-    assert repr(mf.QUADRATIC_EDGES) == "EdgeWeighting('quadratic', ndim=(1, 2, 3), halo=2, degree=2)"
+    assert repr(mf.CUBIC) == ("Weighting('cubic': scatter 1D/2D/3D; gather 1D/2D/3D; halo 2, degree 3, "
+                              "takes clamped axes)")
+    assert repr(mf.QUADRATIC_EDGES) == ("EdgeWeighting('quadratic': gather 1D/2D/3D; deposit_paths 1D/2D/3D; "
+                                        "halo 2, degree 2, takes clamped axes)")
+    assert mf.CUBIC.dimensions() == (1, 2, 3)
+    with pytest.raises(ValueError, match="degree must be >= 1"):
+        mf.EdgeWeighting("bad", gather={}, deposit_paths={}, degree=0)
+    with pytest.raises(ValueError, match=r"the bad edge weighting has no 2D deposit_paths kernel \(has none\)"):
+        mf.EdgeWeighting("bad", gather={}, deposit_paths={}).deposit_paths_kernel(2)
     assert (mf.WHITNEY.degree, mf.QUADRATIC_EDGES.degree, mf.CUBIC_EDGES.degree) == (1, 2, 3)
     with pytest.raises(TypeError):
         mf.LINEAR.scatter[2] = print  # read-only mapping
@@ -175,7 +182,9 @@ def test_splines_pair_the_weightings():
     assert mf.splines(2).nodes is mf.QUADRATIC and mf.splines(2).edges is mf.QUADRATIC_EDGES
     assert mf.splines(3).nodes is mf.CUBIC and mf.splines(3).edges is mf.CUBIC_EDGES
     assert [mf.splines(p).halo for p in (1, 2, 3)] == [1, 2, 2]
-    assert repr(mf.splines(1)) == "Splines(degree=1, nodes='linear', edges='whitney')"
+    assert repr(mf.splines(1)) == "Splines(degree 1: nodes='linear', edges='whitney')"
+    assert mf.splines(1).forms() == (mf.LINEAR, mf.WHITNEY)
+    assert all(w.clamps for w in mf.splines(1, clamped=True).forms())
     with pytest.raises(ValueError, match="no built-in splines of degree 5"):
         mf.splines(5)
     with pytest.raises(ValueError, match="an integer"):

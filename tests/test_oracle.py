@@ -55,7 +55,7 @@ def test_path_oracle_matches_the_reference_numpy_kernels(tag):
 
 # ------------------------------------------------ the reference compiled as C++ --
 
-REF_SRC = Path(os.environ.get("MPF_REFERENCE_SRC", "/root/reference/src")) / "mpifield" / "kernels"
+REF_SRC = Path(os.environ.get("MPF_REFERENCE_SRC", Path(__file__).resolve().parents[2] / "reference" / "src")) / "mpifield" / "kernels"
 needs_ref = pytest.mark.skipif(
     not REF_SRC.is_dir() or not (Path(O.HERE) / "_ref" / "libref_host.so").exists(),
     reason="the mpifield source tree (for oracle/_ref) is not here",
