@@ -20,6 +20,7 @@ __device__ __forceinline__ Grid<double> grid_of(const mpf_batch_request& r) {
         g.lower[d] = r.lower[d];
         g.cell[d] = r.cell[d];
         g.inv[d] = r.inv[d];
+        g.pow2[d] = 0;
         g.num[d] = r.num[d];
         g.code[d] = r.code[d];
         g.ext[d] = r.ext[d];

@@ -118,6 +118,15 @@ static int check_grid(int kind, int degree, int ndim, const double* lower, const
     return MPF_OK;
 }
 
+// Whether c is a power of two whose reciprocal is a normal number of T: then RN(1 / c) is
+// exact and a / c = a * (1 / c) for every a, rounding included.
+template <typename T> static bool exact_reciprocal(T c) {
+    int e = 0;
+    const T m = std::frexp(c, &e);
+    const T r = T(1) / c;
+    return m == T(0.5) && std::isnormal(r) && std::isnormal(c);
+}
+
 template <typename T>
 static Grid<T> make_grid(int ndim, int degree, const double* lower, const double* cell, const int32_t* num,
                          const int32_t* code) {
@@ -127,6 +136,7 @@ static Grid<T> make_grid(int ndim, int degree, const double* lower, const double
         g.lower[d] = on ? (T)lower[d] : T(0);
         g.cell[d] = on ? (T)cell[d] : T(1);
         g.inv[d] = T(1) / g.cell[d];  // host IEEE division in T: RN(1 / cell)
+        g.pow2[d] = exact_reciprocal<T>(g.cell[d]) ? 1 : 0;
         g.num[d] = on ? num[d] : 1;
         g.code[d] = on ? code[d] : PERIODIC;
         g.ext[d] = on ? axis_extent(num[d], code[d], degree) : 1;

@@ -16,6 +16,7 @@ template <typename T> struct Grid {
     int num[3];
     int code[3];
     int ext[3];
+    int pow2[3];  // 1: cell is a power of two, so (x - lower) * inv is the quotient exactly
 };
 
 // A node gather, scatter or position-gradient gather.

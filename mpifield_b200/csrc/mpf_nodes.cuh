@@ -42,7 +42,7 @@ constexpr int kTileScatterMinBlocks = 2;
 
 template <typename T>
 __device__ __forceinline__ T rel_of(const NodeArgs<T>& a, int d, int64_t i) {
-    return div_rn(a.pos[d * a.pos_stride + i] - a.g.lower[d], a.g.cell[d], a.g.inv[d]);
+    return cells_from(a.pos[d * a.pos_stride + i] - a.g.lower[d], a.g.cell[d], a.g.inv[d], a.g.pow2[d]);
 }
 
 // Block-wide min of lo[] and max of hi[] over NDIM axes, into s_lo / s_hi (which the
@@ -359,7 +359,7 @@ __device__ __forceinline__ void drain_and_flag(const NodeArgs<T>& a, uint64_t* b
 
 template <typename T>
 __device__ __forceinline__ T rel_from(const T x, const Grid<T>& g, int d) {
-    return div_rn(x - g.lower[d], g.cell[d], g.inv[d]);
+    return cells_from(x - g.lower[d], g.cell[d], g.inv[d], g.pow2[d]);
 }
 
 // The gather. Positions of chunk k wait in shared buffer k % 2 while the bulk copy of
@@ -971,6 +971,14 @@ __device__ __forceinline__ void flush_clear_box(T* box, T* field, const int* lo,
     });
 }
 
+}  // namespace mpf
+
+// the lean tile kernels (they use the helpers above; the tile scatter below uses their
+// piece walk)
+#include "mpf_runs.cuh"
+
+namespace mpf {
+
 // The tile scatter: the segment scatter (above) for markers sorted by cell tile
 // (mpf_sort_by_tile), one component, every axis periodic. tile_start names the ranks of
 // every tile, so the CTA's share of the ranks (an equal share of the live markers, the
@@ -1232,142 +1240,10 @@ __global__ void __launch_bounds__(BLOCK, MINB) scatter_tiles_kernel(const NodeAr
         for (int q = 0; q < SP; ++q) acc[q] = T(0);
         key = -1;
     }
-}
-
-// ------------------------------------------------------- the tile gather (sorted) --
-
-// The tile gather: the gather for markers sorted by cell tile (mpf_sort_by_tile), every
-// axis periodic. The CTA's share of the live ranks splits at tile boundaries into pieces
-// as in the tile scatter; for each piece the CTA copies the tile's node box (its anchors
-// widened by the stencil, all components) from the field into shared memory once, rows
-// along the last axis read coalesced, and every marker of the piece reads its stencil
-// from there: shared-memory loads of a few neighbouring cells per warp instead of L1
-// loads, and no tag lookups. Markers go to threads in stride (lane l of a warp, marker
-// l of 32 consecutive ones), so position reads and result writes are coalesced. A
-// marker whose anchor is not in the piece's tile reads the field in global memory, so
-// the result never depends on the order.
-template <typename T, int NDIM, int KIND, int P, int NC, int MINB, int TX = 0, int TY = 0, int TZ = 0>
-__global__ void __launch_bounds__(kMaxBlock, MINB) gather_tiles_kernel(const NodeArgs<T> a) {
-    constexpr int S = P + 1;
-    constexpr int H = P / 2;
-    __shared__ TileLoop s_loop;
-    __shared__ TileStep s_step;
-    T* box = reinterpret_cast<T*>(mpf_dynamic_smem);
-    const int t = threadIdx.x;
-    const int tl[3] = {TX > 0 ? TX : a.tile[0], TY > 0 ? TY : a.tile[1], TZ > 0 ? TZ : a.tile[2]};
-    int ex[3] = {1, 1, 1};
-    tile_box_extents<NDIM, P>(tl, ex);
-    // box strides in nodes
-    const int se = NDIM > 2 ? 1 : 0;
-    const int sb = NDIM > 2 ? ex[2] : (NDIM > 1 ? 1 : 0);
-    const int sa = NDIM > 2 ? ex[1] * ex[2] : (NDIM > 1 ? ex[1] : 1);
-    const int st[3] = {sa, NDIM > 1 ? sb : 0, NDIM > 2 ? se : 0};
-    constexpr int L = NDIM - 1;  // the last axis: box rows run along it
-    const int rowlen = ex[L] * NC;
-    int rows = 1;
-#pragma unroll
-    for (int d = 0; d < L; ++d) rows *= ex[d];
-    const int sy = NDIM > 2 ? a.g.ext[2] : 1;
-    const int sx = NDIM > 1 ? a.g.ext[1] * sy : 1;
-    const int gstride[3] = {NDIM == 1 ? 1 : sx, NDIM == 2 ? 1 : sy, 1};
-    if (t == 0) {
-        const int64_t live = min(max(__ldg(a.tile_start + a.ntiles), (int64_t)0), a.n);
-        const int64_t per = (live + gridDim.x - 1) / gridDim.x;
-        s_loop.m = min((int64_t)blockIdx.x * per, live);
-        s_loop.m_end = min(s_loop.m + per, live);
-        s_loop.e = s_loop.m;
-        s_loop.cur = -1;
-        s_loop.sub = s_loop.nsub = 0;
-        s_loop.part = s_loop.extra = 0;
-#pragma unroll
-        for (int d = 0; d < 3; ++d) s_step.blo[d] = s_step.old_lo[d] = 0;
-    }
-    int staged[3] = {INT_MIN, INT_MIN, INT_MIN};  // the first anchor of the tile in the box
-#pragma unroll 1
-    for (;;) {
-        if (t == 0) plan_tile_step<NDIM, H>(s_loop, s_step, a.tile_start, a.ntiles, a.tiles, tl, 1 << 30);
-        // the plan is visible and every thread is done with the box
-        __syncthreads();
-        const int64_t first = s_step.first;
-        const int count = s_step.count;
-        if (count == 0) break;
-        const int blo[3] = {s_step.blo[0], s_step.blo[1], s_step.blo[2]};
-        if (blo[0] != staged[0] || blo[1] != staged[1] || blo[2] != staged[2]) {
-            // the tile's box: row r (the leading axes) of the last axis, entries (node, component)
-            const int lane = t & 31;
-            for (int r = t >> 5; r < rows; r += kMaxBlock / 32) {
-                int rest = r, prefix = 0;
-#pragma unroll
-                for (int d = L - 1; d >= 0; --d) {
-                    const int j = rest % ex[d];
-                    rest /= ex[d];
-                    prefix += map_node(blo[d] - H + j, a.g.num[d], PERIODIC) * gstride[d];
-                }
-                const int z0 = blo[L] - H;
-                for (int e = lane; e < rowlen; e += 32) {
-                    const int j = e / NC;
-                    const int c = e - j * NC;
-                    const int node = prefix + map_node(z0 + j, a.g.num[L], PERIODIC) * gstride[L];
-                    box[r * rowlen + e] = __ldg(a.field_in + (int64_t)node * NC + c);
-                }
-            }
-#pragma unroll
-            for (int d = 0; d < 3; ++d) staged[d] = blo[d];
-            __syncthreads();
-        }
-        // the positions of a thread's next marker are read while it works on the current one
-        T next[3] = {T(0), T(0), T(0)};
-        if (t < count) {
-#pragma unroll
-            for (int d = 0; d < NDIM; ++d) next[d] = __ldg(a.pos + d * a.pos_stride + first + t);
-        }
-#pragma unroll 1
-        for (int j = t; j < count; j += kMaxBlock) {
-            const int64_t i = first + j;
-            T x[3];
-#pragma unroll
-            for (int d = 0; d < 3; ++d) x[d] = next[d];
-            if (j + kMaxBlock < count) {
-#pragma unroll
-                for (int d = 0; d < NDIM; ++d) next[d] = __ldg(a.pos + d * a.pos_stride + i + kMaxBlock);
-            }
-            T w[3][S];
-            int base[3] = {0, 0, 0};
-            int boff[3] = {0, 0, 0};  // the stencil's first node in the box, per axis
-            bool inside = true;
-#pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                if (d < NDIM) {
-                    const T rel = rel_from(x[d], a.g, d);
-                    base[d] = axis_stencil<T, KIND, P>(rel, a.g.num[d], PERIODIC, w[d]);
-                    boff[d] = wrap_index(base[d] + H - blo[d], a.g.num[d]);
-                    inside = inside && (unsigned)boff[d] < (unsigned)tl[d];
-                } else {
-#pragma unroll
-                    for (int z = 0; z < S; ++z) w[d][z] = T(z == 0);
-                }
-            }
-            T acc[NC];
-            if (inside) {  // the box: node (x, y, z) of the stencil at box node offb[0][x] + offb[1][y] + offb[2][z]
-                int offb[3][S];
-#pragma unroll
-                for (int d = 0; d < 3; ++d)
-#pragma unroll
-                    for (int s = 0; s < S; ++s) offb[d][s] = d < NDIM ? (boff[d] + s) * st[d] : 0;
-                stencil_sum<T, NDIM, S, NC, false, int>(box, offb, w, NC, 0, acc);
-            } else {  // not this tile's marker: the field in global memory
-                int off[3][S];
-#pragma unroll
-                for (int d = 0; d < 3; ++d)
-#pragma unroll
-                    for (int s = 0; s < S; ++s)
-                        off[d][s] = d < NDIM ? map_node(base[d] + s, a.g.num[d], PERIODIC) * gstride[d] : 0;
-                stencil_sum<T, NDIM, S, NC, true, int>(a.field_in, off, w, NC, 0, acc);
-            }
-#pragma unroll
-            for (int c = 0; c < NC; ++c) a.result[c * a.res_stride + i] = acc[c];
-        }
-    }
+    // the sentinel tile's ranks (values zero when the store was sorted) through global memory
+    PieceWalk rest;
+    rest.start(a.tile_start, a.ntiles, a.n);
+    scatter_tail<T, NDIM, KIND, P>(a, rest.tail, rest.tail_end, BLOCK);
 }
 
 // The scatter. The markers of a chunk go to warps in contiguous runs of 32 (lane l of

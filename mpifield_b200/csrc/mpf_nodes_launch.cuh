@@ -54,56 +54,49 @@ template <typename T, int NDIM> static int bulk_positions(const NodeArgs<T>& a) 
     return (p % 16 == 0) && (NDIM == 1 || (a.pos_stride * (int64_t)sizeof(T)) % 16 == 0) ? 1 : 0;
 }
 
-// The tile gather (markers sorted by cell tile, periodic axes, 1-3 components): 256
-// threads, kGatherMinBlocks CTAs per SM. Returns MPF_ERR_ARGUMENT, launching nothing, when
-// the tile's node box does not fit that many CTAs' shared memory.
-template <typename T, int NDIM, int KIND, int P, int NC>
-static int run_gather_tiles(NodeArgs<T> a, cudaStream_t stream) {
-    constexpr int MINB = kGatherMinBlocks;
-    int64_t total = NC;
-    for (int d = 0; d < NDIM; ++d) {
-        int64_t e = (int64_t)a.tile[d] + P;
-        if (d == NDIM - 1 && (e & 1) == 0) ++e;
-        total *= e;
-    }
-    const int64_t box_bytes = total * (int64_t)sizeof(T);
-    if (box_bytes > (228 * 1024) / MINB - 2048) return MPF_ERR_ARGUMENT;
-    const int smem = (int)box_bytes;
+// The lean tile gather (mpf_runs.cuh): BLOCK threads, MINB CTAs per SM, BUFFERS boxes.
+// Returns MPF_ERR_ARGUMENT, launching nothing, when the boxes do not fit.
+template <typename T, int NDIM, int KIND, int P, int NC, int BLOCK, int MINB, int BUFFERS>
+static int run_gather_lean(NodeArgs<T> a, cudaStream_t stream) {
+    int64_t box = NC;
+    for (int d = 0; d < NDIM; ++d) box *= (int64_t)a.tile[d] + P;
+    const int64_t bytes = BUFFERS * box * (int64_t)sizeof(T);
+    if (bytes > (228 * 1024) / MINB - 2048) return MPF_ERR_ARGUMENT;
+    const int smem = (int)bytes;
     a.error = device_error_word();
     if (!a.error) return MPF_ERR_CUDA;
-    // the tile shapes of the 3D quadratic stores as compile-time constants, others at run time
-    auto kernel = gather_tiles_kernel<T, NDIM, KIND, P, NC, MINB>;
+    auto kernel = gather_lean_kernel<T, NDIM, KIND, P, NC, 0, 0, 0, BLOCK, MINB, BUFFERS>;
     int shape = 0;
     if constexpr (NDIM == 3 && P == 2) {
         if (a.tile[0] == 8 && a.tile[1] == 8 && a.tile[2] == 8) {
-            kernel = gather_tiles_kernel<T, NDIM, KIND, P, NC, MINB, 8, 8, 8>;
+            kernel = gather_lean_kernel<T, NDIM, KIND, P, NC, 8, 8, 8, BLOCK, MINB, BUFFERS>;
             shape = 1;
-        } else if (a.tile[0] == 8 && a.tile[1] == 8 && a.tile[2] == 16) {
-            kernel = gather_tiles_kernel<T, NDIM, KIND, P, NC, MINB, 8, 8, 16>;
-            shape = 2;
         } else if (a.tile[0] == 4 && a.tile[1] == 4 && a.tile[2] == 64) {
-            kernel = gather_tiles_kernel<T, NDIM, KIND, P, NC, MINB, 4, 4, 64>;
-            shape = 3;
+            kernel = gather_lean_kernel<T, NDIM, KIND, P, NC, 4, 4, 64, BLOCK, MINB, BUFFERS>;
+            shape = 2;
         }
     }
-    static int cache[4][64] = {{0}};
+    static int cache[3][64] = {{0}};
     if (allow_smem(kernel, smem, cache[shape]) != MPF_OK) return MPF_ERR_CUDA;
-    const int64_t units = (a.n + kMaxBlock - 1) / kMaxBlock;
-    kernel<<<grid_for(units, smem, kMaxBlock, MINB), kMaxBlock, smem, stream>>>(a);
+    const int64_t units = (a.n + BLOCK - 1) / BLOCK;
+    kernel<<<grid_for(units, smem, BLOCK, MINB), BLOCK, smem, stream>>>(a);
     count_launches(1);
     return launch_status();
 }
 
-// Gather variants: 0 (default) the tile gather for markers sorted by cell tile (periodic
-// axes, 1-3 components, the tile's node box within shared memory, fewer than 2^31 field
-// entries), else through L1 while the field has fewer than 2^31 entries, else with staged
-// boxes; 1 staged boxes (path 1: global reads in that kernel); 2 through L1.
+// Gather variants for markers sorted by cell tile (periodic axes, 1-3 components, fewer
+// than 2^31 field entries, the tile's box within shared memory): 0 (default) the lean
+// tile gather with one box and three CTAs of 256 per SM, 6 with two boxes and one CTA of
+// 512. Otherwise, and for unsorted markers: through L1 while the field has fewer than
+// 2^31 entries, else with staged boxes; 1 staged boxes (path 1: global reads in that
+// kernel); 2 through L1.
 template <typename T, int NDIM, int KIND, int P, int NC>
 static int run_gather(NodeArgs<T> a, const Tuning& t, cudaStream_t stream) {
     if constexpr (NC > 0) {
-        if (a.tile_start && t.variant == 0 && t.path != 1 && all_periodic<T, NDIM>(a) &&
+        if (a.tile_start && (t.variant == 0 || t.variant == 6) && t.path != 1 && all_periodic<T, NDIM>(a) &&
             field_entries<T, NDIM>(a) < ((int64_t)1 << 31)) {
-            const int st = run_gather_tiles<T, NDIM, KIND, P, NC>(a, stream);
+            const int st = t.variant == 6 ? run_gather_lean<T, NDIM, KIND, P, NC, 512, 1, 2>(a, stream)
+                                          : run_gather_lean<T, NDIM, KIND, P, NC, 256, 3, 1>(a, stream);
             if (st != MPF_ERR_ARGUMENT) return st;
         }
     }
@@ -206,16 +199,58 @@ static int run_scatter_tiles(NodeArgs<T> a, cudaStream_t stream) {
     return launch_status();
 }
 
+// The lean tile scatter (mpf_runs.cuh: coherent lanes, per-warp tables walked by
+// stencil point): BLOCK threads, MINB CTAs per SM. Returns MPF_ERR_ARGUMENT, launching
+// nothing, when the box and the tables do not fit.
+template <typename T, int NDIM, int KIND, int P, int BLOCK, int MINB>
+static int run_scatter_lean(NodeArgs<T> a, cudaStream_t stream) {
+    constexpr int SP = StencilPoints<P + 1, NDIM>::value;
+    int64_t box = 1;
+    for (int d = 0; d < NDIM; ++d) {
+        int64_t e = (int64_t)a.tile[d] + P;
+        if (d == NDIM - 1 && (e & 1) == 0) ++e;
+        box *= e;
+    }
+    const int64_t bytes = (((box + 1) & ~1) + (int64_t)(BLOCK / 32) * 32 * (SP + 2)) * (int64_t)sizeof(T);
+    if (bytes > (228 * 1024) / MINB - 2048) return MPF_ERR_ARGUMENT;
+    const int smem = (int)bytes;
+    a.error = device_error_word();
+    if (!a.error) return MPF_ERR_CUDA;
+    auto kernel = scatter_lean_kernel<T, NDIM, KIND, P, 0, 0, 0, BLOCK, MINB>;
+    int shape = 0;
+    if constexpr (NDIM == 3 && P == 2) {
+        if (a.tile[0] == 8 && a.tile[1] == 8 && a.tile[2] == 8) {
+            kernel = scatter_lean_kernel<T, NDIM, KIND, P, 8, 8, 8, BLOCK, MINB>;
+            shape = 1;
+        } else if (a.tile[0] == 4 && a.tile[1] == 4 && a.tile[2] == 64) {
+            kernel = scatter_lean_kernel<T, NDIM, KIND, P, 4, 4, 64, BLOCK, MINB>;
+            shape = 2;
+        }
+    }
+    static int cache[3][64] = {{0}};
+    if (allow_smem(kernel, smem, cache[shape]) != MPF_OK) return MPF_ERR_CUDA;
+    const int64_t units = (a.n + BLOCK - 1) / BLOCK;
+    kernel<<<grid_for(units, smem, BLOCK, MINB), BLOCK, smem, stream>>>(a);
+    count_launches(1);
+    return launch_status();
+}
+
 // Scatter variants: 0 (default) the tile scatter for markers sorted by cell tile (one
 // component, periodic axes, stencils of at most 27 points, the tile's box within shared
 // memory), else the segment scatter for one component and stencils of at most 27
 // points, else the warp-transposed run reduction; 1 the segment scatter where it
-// applies (tile order ignored); 2 the warp-transposed run reduction.
+// applies (tile order ignored); 2 the warp-transposed run reduction; 5 for markers
+// sorted by cell tile the lean tile scatter (block 128: four CTAs of 128 per SM).
 template <typename T, int NDIM, int KIND, int P, int NC>
 static int run_scatter(NodeArgs<T> a, const Tuning& t, cudaStream_t stream) {
     constexpr int SP = StencilPoints<P + 1, NDIM>::value;
     if constexpr (NC == 1 && SP <= 27) {
-        if (a.tile_start && t.variant == 0 && t.path != 1 && all_periodic<T, NDIM>(a)) {
+        if (a.tile_start && (t.variant == 0 || t.variant == 5) && t.path != 1 && all_periodic<T, NDIM>(a)) {
+            if (t.variant == 5) {
+                const int st = t.block == 128 ? run_scatter_lean<T, NDIM, KIND, P, 128, 4>(a, stream)
+                                              : run_scatter_lean<T, NDIM, KIND, P, 256, 2>(a, stream);
+                if (st != MPF_ERR_ARGUMENT) return st;
+            }
             const int st = run_scatter_tiles<T, NDIM, KIND, P, kSegment, kTileScatterMinBlocks, kTileScatterBlock>(a, stream);
             if (st != MPF_ERR_ARGUMENT) return st;
         }

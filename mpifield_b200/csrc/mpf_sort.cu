@@ -40,7 +40,8 @@ __global__ void tile_keys_kernel(const KeyArgs<T> a) {
         int64_t key = 0, inner = 0;
 #pragma unroll
         for (int d = 0; d < NDIM; ++d) {
-            const T rel = div_rn(a.pos[d * a.pos_stride + i] - a.g.lower[d], a.g.cell[d], a.g.inv[d]);
+            const T rel = cells_from(a.pos[d * a.pos_stride + i] - a.g.lower[d], a.g.cell[d], a.g.inv[d],
+                                     a.g.pow2[d]);
             const int anchor = axis_anchor<T, KIND, P>(rel, a.g.num[d], a.g.code[d]);
             const int t = anchor / a.tile[d];
             key = key * a.ntiles[d] + t;

@@ -62,6 +62,12 @@ template <typename T> __device__ __forceinline__ T div_rn(T a, T b, T rb) {
     return isfinite(q) ? q : a / b;
 }
 
+// a / b, correctly rounded: a * rb when b is a power of two (pow2: rb = 1 / b exactly, so
+// the product is the quotient, rounding included), else div_rn.
+template <typename T> __device__ __forceinline__ T cells_from(T a, T b, T rb, int pow2) {
+    return pow2 ? a * rb : div_rn(a, b, rb);
+}
+
 // rel - num * floor(rel / num): the periodic wrap of the reference stencils.
 template <typename T> __device__ __forceinline__ T wrap_period(T rel, int num) {
     const T n = (T)num;
@@ -154,6 +160,15 @@ __device__ __forceinline__ int clamped_cell(T rel, int num, T* w) {
 // (the weights are uniform_weights<P>(t)).
 template <typename T, int P>
 __device__ __forceinline__ int spline_frame(T rel, int num, int code, T& t) {
+    // the usual case first: a middle node in [1, num - 2] means rel is in [0.5, num - 1.5)
+    // (even P) or [1, num - 1) (odd P), where neither the wrap nor the clamps change anything
+    {
+        const int quick = (P % 2 == 0) ? trunc_int<T>(rel + T(0.5)) : trunc_int<T>(rel);
+        if (quick >= 1 && quick <= num - 2) {
+            t = rel - T(quick);
+            return quick - P / 2;
+        }
+    }
     if (code == PERIODIC) {
         if (!(rel >= T(0) && rel < T(num))) rel = wrap_period(rel, num);
     } else {
@@ -172,6 +187,17 @@ __device__ __forceinline__ int spline_frame(T rel, int num, int code, T& t) {
 template <typename T, int KIND, int P>
 __device__ __forceinline__ int axis_stencil(T rel, int num, int code, T* w) {
     if constexpr (KIND == LINEAR) {
+        // the usual case first: a left node in [1, num - 2] means 1 <= rel < num - 1, where
+        // neither the wrap nor the clamp below changes anything
+        {
+            const int quick = trunc_int<T>(rel);
+            if (quick >= 1 && quick <= num - 2) {
+                const T f = rel - T(quick);
+                w[0] = T(1) - f;
+                w[1] = f;
+                return quick;
+            }
+        }
         int left;
         if (code == PERIODIC) {
             // for 0 < rel < num - 1 the quotient rel / num rounds below 1: the wrap is exact identity
@@ -188,6 +214,15 @@ __device__ __forceinline__ int axis_stencil(T rel, int num, int code, T* w) {
         w[1] = f;
         return left;
     } else if constexpr (KIND == QUADRATIC) {
+        // the usual case first: a nearest node in [1, num - 2] means 0.5 <= rel < num - 1.5,
+        // where neither the wrap nor the clamps below change anything
+        {
+            const int quick = trunc_int<T>(rel + T(0.5));
+            if (quick >= 1 && quick <= num - 2) {
+                uniform_weights<T, 2>(rel - T(quick), w);
+                return quick - 1;
+            }
+        }
         int c;
         if (code == PERIODIC) {
             if (!(rel > T(0) && rel < T(num - 1))) rel = wrap_period(rel, num);
