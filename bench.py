@@ -260,12 +260,11 @@ class Step:
         return t, self.mf.permute(pos, t.order), self.mf.permute(w, t.order)
 
     def gather_scatter(self, pos, w, events=None):
-        """Gather E and scatter the weights on the sorted store (the scatter takes the
-        store's tile starts: mpf_scatter_tiles)."""
-        gather, _ = self.kernels
+        """Gather E and scatter the weights on the sorted store; both take the store's tile
+        starts (mpf_gather_tiles, mpf_scatter_tiles)."""
         if events is not None:
             events[0].record()
-        gather(pos, self.field, self.E, *self.geom)
+        self.mf.kernels.gather(self.lib.QUADRATIC, 2, pos, self.field, self.E, self.geom, order=self.order)
         if events is not None:
             events[1].record()
         self.density.zero_()
@@ -341,6 +340,50 @@ def ref_cuda_time(pos, w, field, density, E, steps: int) -> dict | None:
     t = (g_ms + s_ms) / steps / 1000.0
     return {"value": n / t, "unit": "markers/s", "gather_ms": g_ms / steps, "scatter_ms": s_ms / steps,
             "marker_order": "random", "kernels": "reference gather_quadratic_3d + scatter_quadratic_3d, sm_100a"}
+
+
+def _ref_cuda_lib():
+    """The reference's CUDA kernels compiled for sm_100a from its sources (oracle/_ref), or None."""
+    import ctypes as C
+
+    path = ROOT / "oracle" / "_ref" / "libref_cuda.so"
+    return C.CDLL(str(path)) if path.exists() else None
+
+
+def _ref_call(lib, name: str, n_threads: int, arrays, doubles, ints) -> None:
+    """Launch reference kernel ``name`` (one thread per marker or path, block 256) on torch's
+    current stream: its array views (data, shape, strides in elements), then its double and
+    int arguments, in the order of its signature."""
+    import ctypes as C
+
+    args = [C.c_longlong(n_threads), C.c_int(256), C.c_int(0), C.c_void_p(torch.cuda.current_stream().cuda_stream)]
+    keep = []
+    for t in arrays:
+        shape = (C.c_longlong * t.dim())(*t.shape)
+        strides = (C.c_longlong * t.dim())(*t.stride())
+        keep += [shape, strides]
+        args += [C.c_void_p(t.data_ptr()), shape, strides]
+    args += [C.c_double(float(v)) for v in doubles] + [C.c_int(int(v)) for v in ints]
+    status = getattr(lib, f"refcuda_{name}")(*args)
+    if status != 0:
+        raise RuntimeError(f"reference kernel {name} failed with CUDA error {status}")
+
+
+def _event_stats(fn, reps: int) -> tuple[float, float]:
+    """Mean and best (minimum) milliseconds of ``fn`` over ``reps`` timed calls after one
+    warm-up call, each timed with CUDA events on the current stream (best of N as the
+    reference's examples/12_kernel_backends.py:27-34 reports)."""
+    fn()
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(reps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        fn()
+        b.record()
+        torch.cuda.synchronize()
+        times.append(a.elapsed_time(b))
+    return sum(times) / len(times), min(times)
 
 
 def sorted_sample(sample: int) -> tuple[np.ndarray, np.ndarray]:
@@ -474,7 +517,7 @@ def run_ours(args, world, rank, local) -> None:
         extras["plain_2d"] = measure_plain_2d(device, max(10, args.steps))
         del pos, w
         torch.cuda.empty_cache()
-        extras["autograd"] = measure_autograd(device, reps)
+        extras["autograd"] = measure_autograd(device, reps, peak)
         extras["path_deposit"] = measure_paths(device, reps, peak)
         if args.serve_requests > 0:
             from mpifield_b200 import serving
@@ -550,10 +593,8 @@ def measure_fp32(step, ps, ws, reps: int) -> dict:
     p32, w32, f32 = ps.float(), ws.float(), step.field.float()
     E32 = torch.empty((3, n), dtype=torch.float32, device=ps.device)
     D32 = torch.zeros(step.density.shape, dtype=torch.float32, device=ps.device)
-    gather = mf.KERNELS["gather_quadratic_3d"]
-
     def go():
-        gather(p32, f32, E32, *step.geom)
+        mf.kernels.gather(step.lib.QUADRATIC, 2, p32, f32, E32, step.geom, order=step.order)
         D32.zero_()
         mf.kernels.scatter(step.lib.QUADRATIC, 2, p32, w32, D32, step.geom, order=step.order)
 
@@ -585,10 +626,12 @@ def path_case(device, n: int = 1 << 25, seed: int = 7):
     return start, end, q, grid
 
 
-def measure_paths(device, reps: int, peak: float, n: int = 1 << 25) -> dict:
-    """The path deposit on `path_case`: WHITNEY and QUADRATIC_EDGES, paths in random order
-    and sorted by the start's cell tile; continuity residual max |rho(end) - rho(start) -
-    G^T J| with the node deposit of the same degree."""
+def measure_paths(device, reps: int, peak: float, n: int = 1 << 25, cpu_sample: int | None = 1 << 21) -> dict:
+    """The path deposit on `path_case`: WHITNEY, QUADRATIC_EDGES and CUBIC_EDGES, paths in
+    random order and sorted by the start's cell tile; continuity residual max |rho(end) -
+    rho(start) - G^T J| with the node deposit of the same degree; beside them the
+    reference's CUDA kernels on the same GPU and its CPU kernels on a sample of the paths
+    (``cpu_sample`` None: neither)."""
     import mpifield_b200 as mf
 
     g_n = PATH_GRID
@@ -599,17 +642,46 @@ def measure_paths(device, reps: int, peak: float, n: int = 1 << 25) -> dict:
     edges = torch.zeros((g_n, g_n, g_n, 3), dtype=torch.float64, device=device)
     nbytes = n * 56 + g_n ** 3 * 24 * 2
     out = {"config": f"{g_n}^3 periodic, N={n} paths, |displacement| <= 0.9 cell per axis", "unit": "paths/s",
-           "algorithmic_bytes": nbytes}
-    for degree, name in ((1, "whitney"), (2, "quadratic_edges")):
+           "algorithmic_bytes": nbytes, "timing": "CUDA events, mean and best of the timed repetitions"}
+    ref = _ref_cuda_lib() if cpu_sample is not None else None
+    for degree, name in ((1, "whitney"), (2, "quadratic_edges"), (3, "cubic_edges")):
         ew, nodes = mf.splines(degree).edges, mf.splines(degree).nodes
         res = {}
         for order, (a, b, c) in (("random", (start, end, q)), ("sorted", (s_start, s_end, s_q))):
             def go():
                 edges.zero_()
                 ew.deposit_paths_block(a, b, c[0], edges, grid)
-            ms = _event_ms(go, reps)
-            res[order] = {"value": n / (ms / 1000.0), "ms": ms,
+            ms, best = _event_stats(go, reps)
+            res[order] = {"value": n / (ms / 1000.0), "ms": ms, "best_ms": best,
                           "hbm_frac": nbytes / (ms / 1000.0) / 1e9 / peak}
+        if ref is not None:
+            # the reference's own CUDA deposit (deposit_paths_3d / deposit_paths_spline_3d,
+            # one thread per path) on the same paths and GPU
+            kernel = "deposit_paths_3d" if degree == 1 else "deposit_paths_spline_3d"
+            ints = [g_n] * 3 + [1] * 3 + ([] if degree == 1 else [degree])
+            refs = {}
+            for order, (a, b, c) in (("random", (start, end, q)), ("sorted", (s_start, s_end, s_q))):
+                def go_ref():
+                    edges.zero_()
+                    _ref_call(ref, kernel, n, [a, b, c[0], edges], [0.0] * 3 + [1.0 / g_n] * 3, ints)
+                ms, best = _event_stats(go_ref, max(2, reps // 2))
+                refs[order] = {"value": n / (ms / 1000.0), "ms": ms, "best_ms": best}
+            res["ref_cuda"] = refs
+        if cpu_sample:
+            # the reference's CPU path (its Pyccel kernels restated with OpenMP: WHITNEY on
+            # every host thread, the spline edges serial as the reference runs them)
+            from oracle import oracle as O
+
+            m = cpu_sample if degree == 1 else cpu_sample // 8
+            hs, he, hq = (t[:, :m].cpu().numpy() for t in (start, end, q))
+            host = np.zeros((g_n, g_n, g_n, 3))
+            threads = os.cpu_count() or 1
+            t0 = time.perf_counter()
+            used = O.cpu_deposit(degree, hs, he, hq[0], host, grid.geometry, threads)
+            sec = time.perf_counter() - t0
+            res["cpu"] = {"value": m / sec, "unit": "paths/s", "cores": used or 1, "kind": "port",
+                          "sample": f"{m} paths of the workload"}
+            del host
         before = torch.zeros((g_n, g_n, g_n, 1), dtype=torch.float64, device=device)
         after = torch.zeros_like(before)
         nodes.scatter_block(start, q[0], before, grid)
@@ -625,7 +697,7 @@ def measure_paths(device, reps: int, peak: float, n: int = 1 << 25) -> dict:
     return out
 
 
-def measure_autograd(device, reps: int) -> dict:
+def measure_autograd(device, reps: int, peak: float) -> dict:
     """Differentiation: 512^2 periodic, CUBIC, 1-component field of seeded Fourier modes,
     N = 2^22 uniform markers, weights U[0, 1]; forward + backward of
     sum(w gather(f, x)) + 0.5 ||scatter(x, w)||^2 with respect to f, w and x."""
@@ -656,8 +728,15 @@ def measure_autograd(device, reps: int) -> dict:
             loss = (w * AG.gather(f, x, mf.CUBIC, geom)).sum() + 0.5 * (rho * rho).sum()
             loss.backward()
 
-        ms = _event_ms(go, reps)
-        out[name] = {"value": n / (ms / 1000.0), "ms_per_step": ms}
+        ms, best = _event_stats(go, reps)
+        # compulsory bytes of the step: every pass over the markers (forward gather and
+        # scatter, backward gather, scatter and position gradient) reads positions and one
+        # marker row and writes one; plus a few passes over the 512^2 grid
+        item = 8 if dtype == torch.float64 else 4
+        nbytes = n * 9 * item + 8 * g_n * g_n * item
+        out[name] = {"value": n / (ms / 1000.0), "ms_per_step": ms, "best_ms": best,
+                     "algorithmic_bytes": nbytes, "hbm_frac": nbytes / (ms / 1000.0) / 1e9 / peak}
+    out["reference"] = "none: the reference has no differentiation"
     return out
 
 
@@ -741,10 +820,41 @@ def measure_plain_2d(device, reps: int) -> dict:
     torch.cuda.synchronize()
     same = bool(torch.equal(out_e, expected[1])) and float((rho - expected[0]).abs().max()) <= 1e-12 * float(
         expected[0].abs().max())
-    return {"value": n / (ms / 1000.0), "unit": "markers/s", "us_per_step": ms * 1000.0,
-            "graph_us_per_step": graph_ms * 1000.0, "graph_matches": same,
-            "config": "101x51 bounded, LINEAR, N=100000: scatter + gather (launch-bound); graph_us_per_step: "
-                      "the step replayed from a CUDA graph"}
+    _, best_ms = _event_stats(go, reps)
+    result = {"value": n / (ms / 1000.0), "unit": "markers/s", "us_per_step": ms * 1000.0,
+              "best_us_per_step": best_ms * 1000.0, "graph_us_per_step": graph_ms * 1000.0, "graph_matches": same,
+              "config": "101x51 bounded, LINEAR, N=100000: scatter + gather (launch-bound); graph_us_per_step: "
+                        "the step replayed from a CUDA graph"}
+    ref = _ref_cuda_lib()
+    if ref is not None:
+        # the reference's CUDA scatter_linear_2d + gather_linear_2d on the same arrays and GPU
+        doubles, ints = [0.0, 0.0, geom[2], geom[3]], [nx, ny, 0, 0]
+
+        def go_ref():
+            rho.zero_()
+            _ref_call(ref, "scatter_linear_2d", n, [pos, ones, rho], doubles, ints)
+            _ref_call(ref, "gather_linear_2d", n, [pos, E, out_e], doubles, ints)
+
+        ref_ms, ref_best = _event_stats(go_ref, reps)
+        result["ref_cuda"] = {"value": n / (ref_ms / 1000.0), "us_per_step": ref_ms * 1000.0,
+                              "best_us_per_step": ref_best * 1000.0}
+    # the reference's CPU kernels (OpenMP restatement of its Pyccel versions), all host threads
+    from oracle import oracle as O
+
+    threads = os.cpu_count() or 1
+    hp, hE = pos.cpu().numpy(), E.cpu().numpy()
+    hrho = np.zeros((nx, ny, 1))
+    O.cpu_gather("linear", 1, hp, hE, geom, threads)
+    cpu = []
+    for _ in range(5):
+        t0 = time.perf_counter()
+        hrho[...] = 0.0
+        O.cpu_scatter("linear", 1, hp, np.ones((1, n)), hrho, geom, threads)
+        O.cpu_gather("linear", 1, hp, hE, geom, threads)
+        cpu.append(time.perf_counter() - t0)
+    result["cpu"] = {"value": n / min(cpu), "us_per_step": min(cpu) * 1e6, "cores": threads, "kind": "port",
+                     "sample": "the whole workload, best of 5"}
+    return result
 
 
 def run_reference(args, world, rank) -> None:
@@ -794,7 +904,8 @@ def main() -> None:
             torch.cuda.set_device(device)
             if rank == 0:
                 peak, _ = read_peak()
-                print(json.dumps({"path_deposit": measure_paths(device, max(1, args.steps), peak, args.paths_only)}))
+                print(json.dumps({"path_deposit": measure_paths(device, max(1, args.steps), peak, args.paths_only,
+                                                                cpu_sample=None)}))
             return
         if args.impl == "reference":
             run_reference(args, world, rank)

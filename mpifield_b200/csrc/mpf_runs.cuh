@@ -384,15 +384,17 @@ __global__ void __launch_bounds__(BLOCK, MINB) scatter_lean_kernel(const NodeArg
             const int following = __shfl_down_sync(FULL, key, 1);
             const unsigned ends = __ballot_sync(FULL, lane == 31 || following != key);
             __syncwarp();
-            T acc = T(0);
+            // four partial sums (rows r mod 4) keep the adds of a long run independent
+            T acc[4] = {T(0), T(0), T(0), T(0)};
             const T* col = table + (lane < SP ? lane : 0);
 #pragma unroll
             for (int r = 0; r < 32; ++r) {
-                acc += col[r * PITCH];
+                acc[r & 3] += col[r * PITCH];
                 if (ends & (1u << r)) {
                     const int at = __shfl_sync(FULL, key, r);
-                    if (lane < SP && at >= 0) atomicAdd(box + at + off, acc);
-                    acc = T(0);
+                    if (lane < SP && at >= 0) atomicAdd(box + at + off, (acc[0] + acc[1]) + (acc[2] + acc[3]));
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) acc[q] = T(0);
                 }
             }
             __syncwarp();  // the table is read before the next step writes it

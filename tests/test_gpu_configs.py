@@ -1,8 +1,8 @@
 """Oracle parity at the exact configurations the bench times, through the bench's own code.
 
 - 3D QUADRATIC gather + scatter: 256^3 periodic, a 3-component Fourier field, N = 2^26
-  markers (80% uniform, 20% beam), the store sorted by 4 x 4 x 64 cell tiles, the gather
-  through L1 and the tile scatter with the store's tile starts (`bench.Step`). The sort is
+  markers (80% uniform, 20% beam), the store sorted by 4 x 4 x 64 cell tiles, the tile
+  gather and the tile scatter with the store's tile starts (`bench.Step`). The sort is
   checked bit for bit against the oracle's keys and numpy's stable argsort, E on a random
   subset of 2^20 markers (the gather is independent per marker) and the density of all
   2^26 markers against the oracle, within 1e-12 of max; the float32 variant within its
@@ -88,7 +88,7 @@ def test_c2_float32_variant_within_its_stated_bound(c2_store):
     p32, w32, f32 = ps.float(), ws.float(), step.field.float()
     E32 = torch.empty((3, N_C2), dtype=torch.float32, device=ps.device)
     D32 = torch.zeros(step.density.shape, dtype=torch.float32, device=ps.device)
-    mf.KERNELS["gather_quadratic_3d"](p32, f32, E32, *step.geom)
+    mf.kernels.gather(step.lib.QUADRATIC, 2, p32, f32, E32, step.geom, order=step.order)
     mf.kernels.scatter(step.lib.QUADRATIC, 2, p32, w32, D32, step.geom, order=step.order)
     idx = _subset(N_C2, SUBSET, 4)
     expected_e = O.gather("quadratic", 2, ps[:, idx].cpu().numpy(), step.field.cpu().numpy(), bench.geometry())
