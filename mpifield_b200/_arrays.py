@@ -20,7 +20,7 @@ from __future__ import annotations
 
 import contextlib
 import threading
-from dataclasses import dataclass
+from functools import lru_cache
 
 _TYPES = {"<f8": "f8", "<f4": "f4", "<i4": "i4", "<u4": "u4", "<i8": "i8", "|u1": "u1", "<u1": "u1",
           "|i1": "i1"}
@@ -31,20 +31,18 @@ _TORCH_NAMES = {"float64": "f8", "float32": "f4", "int32": "i4", "int64": "i8", 
 _local = threading.local()
 
 
-@dataclass(frozen=True)
 class DeviceArray:
     """A strided view of device memory: ``ptr`` is the address of element (0, ..., 0),
     ``strides`` are in elements. ``source`` is the object it was read from, ``stream``
     the stream its producer named (None: none named), ``device`` the CUDA device index
-    (None: the current one)."""
+    (None: the current one). A plain slotted record: one is made per array and call."""
 
-    ptr: int
-    shape: tuple[int, ...]
-    strides: tuple[int, ...]
-    dtype: str
-    source: object
-    stream: int | None = None
-    device: int | None = None
+    __slots__ = ("ptr", "shape", "strides", "dtype", "source", "stream", "device")
+
+    def __init__(self, ptr: int, shape: tuple, strides: tuple, dtype: str, source: object,
+                 stream: int | None = None, device: int | None = None) -> None:
+        self.ptr, self.shape, self.strides, self.dtype = ptr, shape, strides, dtype
+        self.source, self.stream, self.device = source, stream, device
 
     @property
     def ndim(self) -> int:
@@ -100,25 +98,30 @@ class DeviceArray:
         return base.as_strided(self.shape, self.strides, offset)
 
 
+@lru_cache(maxsize=256)
+def _c_strides(shape: tuple) -> tuple:
+    """The element strides of a C-contiguous array of ``shape``."""
+    strides, step = [], 1
+    for n in reversed(shape):
+        strides.append(step)
+        step *= n
+    return tuple(reversed(strides))
+
+
 def _from_interface(obj, iface: dict) -> DeviceArray:
-    typestr = iface["typestr"]
-    if typestr not in _TYPES:
-        raise TypeError(f"mpifield_b200 kernels take float64 or float32 arrays, got type {typestr!r}")
+    dtype = _TYPES.get(iface["typestr"])
+    if dtype is None:
+        raise TypeError(f"mpifield_b200 kernels take float64 or float32 arrays, got type {iface['typestr']!r}")
     if iface.get("mask") is not None:
         raise TypeError("masked device arrays are not supported")
-    dtype = _TYPES[typestr]
     size = _SIZES[dtype]
-    shape = tuple(int(n) for n in iface["shape"])
-    if iface.get("strides") is None:
-        strides, step = [], 1
-        for n in reversed(shape):
-            strides.append(step)
-            step *= n
-        strides = tuple(reversed(strides))
+    shape = tuple(iface["shape"])
+    raw = iface.get("strides")
+    if raw is None:
+        strides = _c_strides(shape)
     else:
-        raw = tuple(int(s) for s in iface["strides"])
         if any(s % size for s in raw):
-            raise ValueError(f"strides {raw} are not whole elements of {size} bytes")
+            raise ValueError(f"strides {tuple(raw)} are not whole elements of {size} bytes")
         strides = tuple(s // size for s in raw)
     ptr = int(iface["data"][0] or 0)
     stream = iface.get("stream") if int(iface.get("version", 2)) >= 3 else None
@@ -132,14 +135,13 @@ def as_device_array(obj, name: str = "array") -> DeviceArray:
         return obj
     torch = _torch_module()
     if torch is not None and isinstance(obj, torch.Tensor):
-        if obj.device.type != "cuda":
+        if not obj.is_cuda:
             raise TypeError(
                 f"mpifield_b200 runs on CUDA device arrays only (no CPU fallback); {name} is on {obj.device}")
-        dtype = _TORCH_NAMES.get(str(obj.dtype).replace("torch.", ""))
+        dtype = _TORCH_DTYPES.get(obj.dtype)
         if dtype is None:
             raise TypeError(f"mpifield_b200 kernels take float64 or float32 arrays, got {obj.dtype}")
-        return DeviceArray(obj.data_ptr(), tuple(obj.shape), tuple(obj.stride()), dtype, obj, None,
-                           obj.device.index)
+        return DeviceArray(obj.data_ptr(), tuple(obj.shape), obj.stride(), dtype, obj, None, obj.get_device())
     iface = getattr(obj, "__cuda_array_interface__", None)
     if iface is not None:
         return _from_interface(obj, iface)
@@ -153,12 +155,24 @@ def as_device_array(obj, name: str = "array") -> DeviceArray:
         f"__cuda_array_interface__ or __dlpack__); {name} is a {type(obj).__name__}")
 
 
+_TORCH = None
+_TORCH_DTYPES: dict = {}
+_RAW_STREAM = None
+
+
 def _torch_module():
-    try:
-        import torch
-    except ImportError:  # pragma: no cover
-        return None
-    return torch
+    """torch (imported once), with its dtype table and its raw current-stream query."""
+    global _TORCH, _RAW_STREAM
+    if _TORCH is None:
+        try:
+            import torch
+        except ImportError:  # pragma: no cover
+            return None
+        for name, code in _TORCH_NAMES.items():
+            _TORCH_DTYPES[getattr(torch, name)] = code
+        _RAW_STREAM = getattr(torch._C, "_cuda_getCurrentRawStream", None)
+        _TORCH = torch
+    return _TORCH
 
 
 def _cupy_stream() -> int | None:
@@ -177,11 +191,14 @@ def launch_stream(*arrays: DeviceArray) -> int:
     for a in arrays:
         if a.stream is not None:
             return a.stream
-    if any(not _is_torch(a.source) for a in arrays):
+    torch = _torch_module()
+    if torch is None or any(not isinstance(a.source, torch.Tensor) for a in arrays):
         cupy = _cupy_stream()
         return 0 if cupy is None else cupy
     torch = _torch_module()
     device = next((a.device for a in arrays if a.device is not None), None)
+    if _RAW_STREAM is not None:
+        return int(_RAW_STREAM(torch.cuda.current_device() if device is None else device))
     return int(torch.cuda.current_stream(device).cuda_stream)
 
 

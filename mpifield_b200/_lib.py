@@ -7,6 +7,7 @@ the library is missing or no CUDA device is present, every call raises.
 from __future__ import annotations
 
 import ctypes as C
+import functools
 import threading
 from pathlib import Path
 
@@ -169,7 +170,13 @@ def stream_of(device: torch.device) -> int:
 
 
 def geometry_arrays(geometry) -> tuple[C.Array, C.Array, C.Array, C.Array, int]:
-    """``(*lower, *cell, *num, *code)`` as C arrays, and ndim."""
+    """``(*lower, *cell, *num, *code)`` as C arrays, and ndim (one set per geometry, kept:
+    the calls only read them)."""
+    return _geometry_arrays(tuple(geometry))
+
+
+@functools.lru_cache(maxsize=1024)
+def _geometry_arrays(geometry: tuple) -> tuple[C.Array, C.Array, C.Array, C.Array, int]:
     if len(geometry) % 4 != 0 or not 4 <= len(geometry) <= 12:
         raise ValueError(f"a geometry has 4 * ndim entries, got {len(geometry)}")
     ndim = len(geometry) // 4

@@ -28,7 +28,9 @@ contiguous copy, as ``cunumpy.kernels.kernel_output`` does for the reference.
 
 from __future__ import annotations
 
+import contextlib
 import ctypes as C
+import functools
 from dataclasses import dataclass
 
 from mpifield_b200 import _lib
@@ -111,6 +113,11 @@ class _Output:
 
 
 def _extent(num, code, degree) -> tuple[int, ...]:
+    return _extent_of(tuple(num), tuple(code), degree)
+
+
+@functools.lru_cache(maxsize=1024)
+def _extent_of(num: tuple, code: tuple, degree: int) -> tuple[int, ...]:
     return tuple(int(n) + (degree - 1 if int(c) == 2 else 0) for n, c in zip(num, code))
 
 
@@ -156,20 +163,17 @@ def _degree(takes_degree: bool, fixed: int | None, args: tuple) -> tuple[int, tu
     return int(fixed), args
 
 
+_NO_STREAM = contextlib.nullcontext()
+
+
 def _launch_options(kernel: str, launch: dict):
+    if not launch:
+        return _NO_STREAM
     unknown = set(launch) - _LAUNCH_KEYWORDS - {"stream"}
     if unknown:
         raise TypeError(f"{kernel} got unexpected keyword arguments {sorted(unknown)}")
     stream = launch.get("stream")
-    return use_stream(stream) if stream is not None else _NoStream()
-
-
-class _NoStream:
-    def __enter__(self):
-        return None
-
-    def __exit__(self, *exc):
-        return False
+    return use_stream(stream) if stream is not None else _NO_STREAM
 
 
 @dataclass(frozen=True)
