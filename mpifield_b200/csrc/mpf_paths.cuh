@@ -483,8 +483,8 @@ __device__ __forceinline__ bool path_cells(const PathArgs<T>& a, int64_t i, T* r
     for (int d = 0; d < NDIM; ++d) {
         const T s = a.start[d * a.start_stride + i];
         const T e = a.end[d * a.end_stride + i];
-        r0[d] = (s - a.g.lower[d]) / a.g.cell[d];
-        r1[d] = (e - a.g.lower[d]) / a.g.cell[d];
+        r0[d] = cells_from(s - a.g.lower[d], a.g.cell[d], a.g.inv[d], a.g.pow2[d]);
+        r1[d] = cells_from(e - a.g.lower[d], a.g.cell[d], a.g.inv[d], a.g.pow2[d]);
         if constexpr (WHITNEY) {
             const T big = sizeof(T) == 8 ? T(1e300) : T(3e38);
             if (!(r0[d] > -big && r0[d] < big && r1[d] > -big && r1[d] < big)) finite = false;
@@ -710,33 +710,27 @@ __global__ void __launch_bounds__(256) deposit_paths_tiled_kernel(const PathArgs
     if (have_box) flush_edge_box<T, NDIM>(tile, a.edges_out, sink, a.g);
 }
 
-// One thread per path, global atomics; BLOCK threads, at least MINB CTAs per SM.
+// One thread per path, global atomics; BLOCK threads, at least MINB CTAs per SM. Each CTA
+// takes an equal contiguous share of the paths, BLOCK consecutive paths at a time, so that
+// in a store sorted by cell the CTAs work in different regions of the grid at once and
+// their atomic adds spread over the L2 (a grid-stride walk keeps every CTA in one small
+// region of a sorted store). Lane l of warp w takes the path l * (BLOCK / 32) + w of
+// the BLOCK: the lanes of a warp are BLOCK / 32 paths apart, in different cells, so the
+// adds of one instruction do not pile onto the same edges.
 template <typename T, int NDIM, int P, bool WHITNEY, int BLOCK = 256, int MINB = 1>
 __global__ void __launch_bounds__(BLOCK, MINB) deposit_paths_kernel(const PathArgs<T> a) {
     GlobalEdgeSink<T, NDIM> sink;
     sink.edges = a.edges_out;
 #pragma unroll
     for (int d = 0; d < 3; ++d) sink.ext[d] = a.g.ext[d];
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.n;
-         i += (int64_t)gridDim.x * blockDim.x) {
+    const int slot = (threadIdx.x & 31) * (BLOCK / 32) + (threadIdx.x >> 5);
+    const int64_t per = ((a.n + gridDim.x - 1) / gridDim.x + BLOCK - 1) / BLOCK * BLOCK;
+    const int64_t mine_end = min(a.n, (int64_t)(blockIdx.x + 1) * per);
+    for (int64_t i = (int64_t)blockIdx.x * per + slot; i < mine_end; i += BLOCK) {
         const T q = a.charges[i];
         if (q == T(0)) continue;
         T r0[NDIM], r1[NDIM];
-        bool finite = true;
-#pragma unroll
-        for (int d = 0; d < NDIM; ++d) {
-            const T s = a.start[d * a.start_stride + i];
-            const T e = a.end[d * a.end_stride + i];
-            r0[d] = (s - a.g.lower[d]) / a.g.cell[d];
-            r1[d] = (e - a.g.lower[d]) / a.g.cell[d];
-            if constexpr (WHITNEY) {
-                const T big = sizeof(T) == 8 ? T(1e300) : T(3e38);
-                if (!(r0[d] > -big && r0[d] < big && r1[d] > -big && r1[d] < big)) finite = false;
-            } else {
-                if (!(s - s == T(0)) || !(e - e == T(0))) finite = false;
-            }
-        }
-        if (!finite) continue;
+        if (!path_cells<T, NDIM, WHITNEY>(a, i, r0, r1)) continue;
         if constexpr (WHITNEY) whitney_path<T, NDIM>(q, r0, r1, a.g, sink);
         else spline_path<T, NDIM, P>(q, r0, r1, a.g, sink);
     }
@@ -751,7 +745,7 @@ __global__ void __launch_bounds__(256) gather_edges_kernel(const PathArgs<T> a) 
         T rel[NDIM];
 #pragma unroll
         for (int d = 0; d < NDIM; ++d) {
-            rel[d] = (a.pos[d * a.pos_stride + i] - a.g.lower[d]) / a.g.cell[d];
+            rel[d] = cells_from(a.pos[d * a.pos_stride + i] - a.g.lower[d], a.g.cell[d], a.g.inv[d], a.g.pow2[d]);
             if (!WHITNEY && a.g.code[d] != PERIODIC) {
                 const T top = T(a.g.num[d] - 1);
                 if (rel[d] < T(0)) rel[d] = T(0);
