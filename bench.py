@@ -386,6 +386,60 @@ def _event_stats(fn, reps: int) -> tuple[float, float]:
     return sum(times) / len(times), min(times)
 
 
+def measure_steady(step, ps, ws, reps: int) -> dict:
+    """The steady state of a particle-in-cell store kept sorted across steps: every step
+    pushes the markers (a fixed displacement of up to 0.3 cell per axis, per rank), re-sorts
+    the store against its previous sorted keys (mpf_resort_by_tile: only the markers whose
+    cell changed are sorted), permutes positions and weights, and gathers and scatters on
+    the new order. The last step's order is checked against a full sort of the store."""
+    mf = step.mf
+    saved = step.order
+    g = torch.Generator(device=ps.device).manual_seed(9)
+    disp = (torch.rand(ps.shape, generator=g, device=ps.device, dtype=ps.dtype) * 0.6 - 0.3) / GRID
+    pos, w = ps.clone(), ws.clone()
+    t = mf.resort_by_tile(pos, mf.QUADRATIC, step.geom, TILE, within=True)
+    pos, w = mf.permute(pos, t.order), mf.permute(w, t.order)
+    spare = [torch.empty_like(pos), torch.empty_like(w)]
+    state = {"pos": pos, "w": w, "t": t}
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+
+    def one(events=None):
+        pos, w = state["pos"], state["w"]
+        pos.add_(disp).remainder_(1.0)
+        if events:
+            events[0].record()
+        t = mf.resort_by_tile(pos, mf.QUADRATIC, step.geom, TILE, within=True, previous=state["t"])
+        mf.permute(pos, t.order, out=spare[0])
+        mf.permute(w, t.order, out=spare[1])
+        if events:
+            events[1].record()
+        state["pos"], spare[0] = spare[0], pos
+        state["w"], spare[1] = spare[1], w
+        state["t"] = t
+        step.order = t
+        step.gather_scatter(state["pos"], state["w"])
+        if events:
+            events[2].record()
+
+    ms = _event_ms(one, reps)
+    resort = []
+    for _ in range(max(2, reps // 4)):
+        one(ev)
+        torch.cuda.synchronize()
+        resort.append(ev[0].elapsed_time(ev[1]))
+    full = mf.sort_by_tile(state["pos"], mf.QUADRATIC, step.geom, TILE, within=True)
+    same = bool(torch.equal(full.order, state["t"].order)) and bool(torch.equal(full.tile_start, state["t"].tile_start))
+    moved = float((state["t"].sorted_keys != state["t"].sorted_keys).sum())  # zero: a shape check of the keys
+    step.order = saved
+    n = ps.shape[1]
+    del disp, spare, state
+    torch.cuda.empty_cache()
+    return {"value": n / (ms / 1000.0), "unit": "markers/s", "ms_per_step": ms,
+            "resort_and_permute_ms": sum(resort) / len(resort), "order_equals_full_sort": same and moved == 0.0,
+            "what": "push (up to 0.3 cell per axis) + incremental re-sort against the previous sorted keys + "
+                    "permute positions and weights + gather + scatter, the store kept in cell-tile order"}
+
+
 def sorted_sample(sample: int) -> tuple[np.ndarray, np.ndarray]:
     """A sample of the workload's markers in the store's cell-tile order."""
     from oracle import oracle as O
@@ -512,6 +566,7 @@ def run_ours(args, world, rank, local) -> None:
     extras = {}
     if not args.no_extras and rank == 0 and world == 1 and dtype == torch.float64:
         reps = max(2, args.steps // 2)
+        extras["steady_step"] = measure_steady(step, ps, ws, reps)
         extras["fp32_variant"] = measure_fp32(step, ps, ws, reps)
         extras["deterministic_scatter"] = measure_deterministic(step, ps, ws, reps)
         extras["plain_2d"] = measure_plain_2d(device, max(10, args.steps))

@@ -282,6 +282,32 @@ MPF_API int mpf_sort_by_tile(int kind, int degree, int ndim, const void* positio
                      int dtype, void* stream);
 
 /*
+ * The cell-tile sort of a store that is kept sorted: the markers' keys as in
+ * mpf_sort_by_tile, computed from the positions (and values) in the store's current
+ * order; order[j] is the current rank of the marker of new rank j in the stable
+ * ascending order of the keys (numpy.argsort(keys, kind="stable"), bit for bit), tile_start
+ * as in mpf_sort_by_tile, and sorted_keys[j] the key of rank j -- what the next call takes
+ * as prev_sorted_keys once the store's arrays have been permuted by order
+ * (mpf_permute_rows). With prev_sorted_keys NULL it is a full sort; with the sorted keys
+ * this call returned for the store before its markers moved, only the markers whose key
+ * changed are sorted and merged with the others (the order is the same): after a step
+ * in which markers move less than a cell, a fraction of the full sort's cost.
+ * prev_sorted_keys must be exactly those keys, and must not be sorted_keys. `workspace`
+ * holds `mpf_resort_workspace_bytes` bytes of device memory, 256-byte aligned. No
+ * reference kernel sorts (picnic's sort_by_cell keeps the reference's stores sorted,
+ * src/mpifield/kernels/scatter_linear_3d/scatter_linear_3d_pyccel.py:11-12).
+ */
+MPF_API int mpf_resort_workspace_bytes(int kind, int degree, int ndim, const int32_t* num, const int32_t* code,
+                                       const int32_t* tile, int within, int64_t n, size_t* bytes);
+MPF_API int mpf_resort_by_tile(int kind, int degree, int ndim, const void* positions, int64_t pos_stride,
+                               const void* values, int64_t val_stride, int64_t ncomp, int64_t n,
+                               const double* lower, const double* cell, const int32_t* num,
+                               const int32_t* code, const int32_t* tile, int within,
+                               const uint32_t* prev_sorted_keys, uint32_t* sorted_keys, int32_t* order,
+                               int64_t* tile_start, void* workspace, size_t workspace_bytes, int dtype,
+                               void* stream);
+
+/*
  * mpf_sort_by_tile without a workspace argument and without any allocation. No
  * counterpart in the reference. It is for callers that cannot call cudaMalloc: a host
  * application that gives all device memory to its own pool or arena at start-up and

@@ -14,13 +14,13 @@ from mpifield_b200._types import BlockGrid, Bounds
 from mpifield_b200.edges import CUBIC_EDGES, QUADRATIC_EDGES, WHITNEY, EdgeWeighting
 from mpifield_b200.field import Field
 from mpifield_b200.kernels import KERNELS
-from mpifield_b200.sorting import TileOrder, permute, sort_by_tile, unpermute
+from mpifield_b200.sorting import TileOrder, permute, resort_by_tile, sort_by_tile, unpermute
 from mpifield_b200.splines import CLAMPED_SPLINES, SPLINES, Splines, splines
 from mpifield_b200.weighting import CUBIC, LINEAR, QUADRATIC, Weighting, spline_weighting
 
 __all__ = [
     "BlockGrid", "Bounds", "CLAMPED_SPLINES", "CUBIC", "CUBIC_EDGES", "EdgeWeighting", "Field", "KERNELS",
     "LINEAR", "QUADRATIC", "QUADRATIC_EDGES", "SPLINES", "Splines", "TileOrder", "WHITNEY", "Weighting",
-    "permute", "sort_by_tile", "spline_weighting", "splines", "unpermute", "use_stream",
+    "permute", "resort_by_tile", "sort_by_tile", "spline_weighting", "splines", "unpermute", "use_stream",
 ]
 __version__ = "1.0.0"

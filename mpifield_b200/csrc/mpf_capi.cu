@@ -607,6 +607,38 @@ int check_sort_arguments(int kind, int degree, int ndim, const void* positions, 
     return MPF_OK;
 }
 
+// The cell-tile keys of the markers (tile_keys_kernel), arguments already checked.
+int compute_keys(int kind, int degree, int ndim, const void* positions, int64_t pos_stride, const void* values,
+                 int64_t val_stride, int64_t ncomp, int64_t n, const double* lower, const double* cell,
+                 const int32_t* num, const int32_t* code, const int32_t* tile, int within, int64_t ntiles,
+                 int64_t cells, uint32_t* keys, int dtype, cudaStream_t s) {
+    if (n == 0) return MPF_OK;
+    if (dtype == MPF_F64) {
+        KeyArgs<double> a;
+        std::memset(&a, 0, sizeof(a));
+        a.g = make_grid<double>(ndim, degree, lower, cell, num, code);
+        a.pos = (const double*)positions; a.pos_stride = pos_stride;
+        a.values = (const double*)values; a.val_stride = val_stride; a.ncomp = ncomp; a.n = n;
+        for (int d = 0; d < 3; ++d) {
+            a.tile[d] = d < ndim ? tile[d] : 1;
+            a.ntiles[d] = d < ndim ? (a.g.ext[d] + a.tile[d] - 1) / a.tile[d] : 1;
+        }
+        a.sentinel = (uint32_t)(ntiles * cells); a.within = within; a.keys = keys;
+        return tile_keys<double>(kind, degree, ndim, a, s);
+    }
+    KeyArgs<float> a;
+    std::memset(&a, 0, sizeof(a));
+    a.g = make_grid<float>(ndim, degree, lower, cell, num, code);
+    a.pos = (const float*)positions; a.pos_stride = pos_stride;
+    a.values = (const float*)values; a.val_stride = val_stride; a.ncomp = ncomp; a.n = n;
+    for (int d = 0; d < 3; ++d) {
+        a.tile[d] = d < ndim ? tile[d] : 1;
+        a.ntiles[d] = d < ndim ? (a.g.ext[d] + a.tile[d] - 1) / a.tile[d] : 1;
+    }
+    a.sentinel = (uint32_t)(ntiles * cells); a.within = within; a.keys = keys;
+    return tile_keys<float>(kind, degree, ndim, a, s);
+}
+
 }  // namespace mpf
 extern "C" {
 
@@ -621,36 +653,41 @@ int mpf_sort_by_tile(int kind, int degree, int ndim, const void* positions, int6
     if (workspace_bytes < sort_workspace_bytes(n) || (!workspace && n > 0)) return MPF_ERR_WORKSPACE;
     if ((reinterpret_cast<uintptr_t>(workspace) % 256) != 0) return MPF_ERR_ALIGNMENT;
     const cudaStream_t s = static_cast<cudaStream_t>(stream);
-    if (n > 0) {
-        int st;
-        if (dtype == MPF_F64) {
-            KeyArgs<double> a;
-            std::memset(&a, 0, sizeof(a));
-            a.g = make_grid<double>(ndim, degree, lower, cell, num, code);
-            a.pos = (const double*)positions; a.pos_stride = pos_stride;
-            a.values = (const double*)values; a.val_stride = val_stride; a.ncomp = ncomp; a.n = n;
-            for (int d = 0; d < 3; ++d) {
-                a.tile[d] = d < ndim ? tile[d] : 1;
-                a.ntiles[d] = d < ndim ? (a.g.ext[d] + a.tile[d] - 1) / a.tile[d] : 1;
-            }
-            a.sentinel = (uint32_t)(ntiles * cells); a.within = within; a.keys = keys;
-            st = tile_keys<double>(kind, degree, ndim, a, s);
-        } else {
-            KeyArgs<float> a;
-            std::memset(&a, 0, sizeof(a));
-            a.g = make_grid<float>(ndim, degree, lower, cell, num, code);
-            a.pos = (const float*)positions; a.pos_stride = pos_stride;
-            a.values = (const float*)values; a.val_stride = val_stride; a.ncomp = ncomp; a.n = n;
-            for (int d = 0; d < 3; ++d) {
-                a.tile[d] = d < ndim ? tile[d] : 1;
-                a.ntiles[d] = d < ndim ? (a.g.ext[d] + a.tile[d] - 1) / a.tile[d] : 1;
-            }
-            a.sentinel = (uint32_t)(ntiles * cells); a.within = within; a.keys = keys;
-            st = tile_keys<float>(kind, degree, ndim, a, s);
-        }
-        if (st != MPF_OK) return st;
-    }
+    MPF_TRY(compute_keys(kind, degree, ndim, positions, pos_stride, values, val_stride, ncomp, n, lower, cell, num,
+                         code, tile, within, ntiles, cells, keys, dtype, s));
     return sort_keys(keys, n, ntiles, cells, order, tile_start, workspace, s);
+}
+
+int mpf_resort_workspace_bytes(int kind, int degree, int ndim, const int32_t* num, const int32_t* code,
+                               const int32_t* tile, int within, int64_t n, size_t* bytes) {
+    if (!bytes || n < 0 || n > INT32_MAX || (within != 0 && within != 1)) return MPF_ERR_ARGUMENT;
+    int64_t ntiles = 0;
+    MPF_TRY(mpf_num_tiles(kind, degree, ndim, num, code, tile, &ntiles));
+    int64_t cells = 1;
+    if (within)
+        for (int d = 0; d < ndim; ++d) cells *= tile[d];
+    *bytes = resort_workspace_bytes(n, ntiles * cells + 1);
+    return MPF_OK;
+}
+
+int mpf_resort_by_tile(int kind, int degree, int ndim, const void* positions, int64_t pos_stride,
+                       const void* values, int64_t val_stride, int64_t ncomp, int64_t n, const double* lower,
+                       const double* cell, const int32_t* num, const int32_t* code, const int32_t* tile, int within,
+                       const uint32_t* prev_sorted_keys, uint32_t* sorted_keys, int32_t* order, int64_t* tile_start,
+                       void* workspace, size_t workspace_bytes, int dtype, void* stream) {
+    int64_t ntiles = 0, cells = 1;
+    MPF_TRY(check_sort_arguments(kind, degree, ndim, positions, pos_stride, values, val_stride, ncomp, n, lower,
+                                 cell, num, code, tile, within, sorted_keys, order, tile_start, dtype, &ntiles,
+                                 &cells));
+    if (workspace_bytes < resort_workspace_bytes(n, ntiles * cells + 1) || (!workspace && n > 0))
+        return MPF_ERR_WORKSPACE;
+    if ((reinterpret_cast<uintptr_t>(workspace) % 256) != 0) return MPF_ERR_ALIGNMENT;
+    if (prev_sorted_keys && prev_sorted_keys == sorted_keys) return MPF_ERR_ARGUMENT;
+    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    uint32_t* keys = n > 0 ? resort_keys_buffer(workspace, n) : nullptr;
+    MPF_TRY(compute_keys(kind, degree, ndim, positions, pos_stride, values, val_stride, ncomp, n, lower, cell, num,
+                         code, tile, within, ntiles, cells, keys, dtype, s));
+    return resort_keys(n, ntiles, cells, prev_sorted_keys, sorted_keys, order, tile_start, workspace, s);
 }
 
 int mpf_permute_rows(void* dst, int64_t dst_stride, const void* src, int64_t src_stride, int64_t rows,

@@ -123,11 +123,20 @@ int sort_keys(const uint32_t* keys, int64_t n, int64_t num_tiles, int64_t cells,
               int64_t* tile_start, void* workspace, cudaStream_t stream);
 int permute_rows(void* dst, int64_t ds, const void* src, int64_t ss, int64_t rows, const int32_t* order,
                  int64_t n, int dtype, cudaStream_t stream);
+size_t resort_workspace_bytes(int64_t n, int64_t nkeys);
+uint32_t* resort_keys_buffer(void* workspace, int64_t n);
+int resort_keys(int64_t n, int64_t num_tiles, int64_t cells, const uint32_t* prev_sorted, uint32_t* sorted_out,
+                int32_t* order, int64_t* tile_start, void* workspace, cudaStream_t stream);
 
 int unpermute_rows(void* dst, int64_t ds, const void* src, int64_t ss, int64_t rows, const int32_t* order,
                    int64_t n, int dtype, cudaStream_t stream);
 
 int sm_count();
+
+int compute_keys(int kind, int degree, int ndim, const void* positions, int64_t pos_stride, const void* values,
+                 int64_t val_stride, int64_t ncomp, int64_t n, const double* lower, const double* cell,
+                 const int32_t* num, const int32_t* code, const int32_t* tile, int within, int64_t ntiles,
+                 int64_t cells, uint32_t* keys, int dtype, cudaStream_t s);
 
 int check_sort_arguments(int kind, int degree, int ndim, const void* positions, int64_t& pos_stride,
                          const void* values, int64_t& val_stride, int64_t ncomp, int64_t n, const double* lower,

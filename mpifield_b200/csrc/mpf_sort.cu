@@ -58,9 +58,10 @@ __global__ void tile_keys_kernel(const KeyArgs<T> a) {
 }
 
 template <int BITS>
-__global__ void digit_histogram_kernel(const uint32_t* keys, int64_t n, int shift, uint32_t* counts,
-                                       int64_t nblocks) {
+__global__ void digit_histogram_kernel(const uint32_t* keys, int64_t n, const int64_t* n_dev, int shift,
+                                       uint32_t* counts, int64_t nblocks) {
     constexpr int DIGITS = 1 << BITS;
+    if (n_dev) n = min(n, *n_dev);  // the count known on the device only (a mover sort)
     __shared__ uint32_t hist[DIGITS];
     for (int d = threadIdx.x; d < DIGITS; d += blockDim.x) hist[d] = 0;
     __syncthreads();
@@ -149,9 +150,10 @@ __global__ void scan_chunks_kernel(uint32_t* data, int64_t count, const uint32_t
 // memory (kWarps << BITS words) and become the warps' output offsets in place.
 template <int BITS>
 __global__ void digit_scatter_kernel(const uint32_t* keys_in, const int32_t* vals_in, int64_t n,
-                                     int shift, const uint32_t* offsets, int64_t nblocks,
+                                     const int64_t* n_dev, int shift, const uint32_t* offsets, int64_t nblocks,
                                      uint32_t* keys_out, int32_t* vals_out) {
     constexpr int DIGITS = 1 << BITS;
+    if (n_dev) n = min(n, *n_dev);
     extern __shared__ uint32_t warp_count[];  // [kWarps][DIGITS]
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
@@ -309,9 +311,10 @@ int tile_keys(int kind, int degree, int ndim, const KeyArgs<T>& a, cudaStream_t 
 }
 
 template <int BITS>
-static int radix_pass(const uint32_t* kin, const int32_t* vin, int64_t n, int shift, uint32_t* counts,
-                      uint32_t* sums, int64_t nb, uint32_t* kout, int32_t* vout, cudaStream_t stream) {
-    digit_histogram_kernel<BITS><<<(unsigned)nb, kSortBlock, 0, stream>>>(kin, n, shift, counts, nb);
+static int radix_pass(const uint32_t* kin, const int32_t* vin, int64_t n, const int64_t* n_dev, int shift,
+                      uint32_t* counts, uint32_t* sums, int64_t nb, uint32_t* kout, int32_t* vout,
+                      cudaStream_t stream) {
+    digit_histogram_kernel<BITS><<<(unsigned)nb, kSortBlock, 0, stream>>>(kin, n, n_dev, shift, counts, nb);
     count_launches(1);
     if (launch_status() != MPF_OK) return MPF_ERR_CUDA;
     const int st = scan_exclusive(counts, nb << BITS, sums, stream);
@@ -324,21 +327,20 @@ static int radix_pass(const uint32_t* kin, const int32_t* vin, int64_t n, int sh
             return MPF_ERR_CUDA;
         configured = smem;
     }
-    digit_scatter_kernel<BITS><<<(unsigned)nb, kSortBlock, smem, stream>>>(kin, vin, n, shift, counts, nb, kout, vout);
+    digit_scatter_kernel<BITS><<<(unsigned)nb, kSortBlock, smem, stream>>>(kin, vin, n, n_dev, shift, counts, nb,
+                                                                          kout, vout);
     count_launches(1);
     return launch_status();
 }
 
-// Sort (keys, marker) pairs stably; the marker order lands in `order`, the tile starts
-// in `tile_start`. Keys are below max_key + 1 (max_key, the sentinel, included); the
-// passes take 8 to 10 bits each, as few passes as 10-bit digits allow.
-int sort_keys(const uint32_t* keys, int64_t n, int64_t num_tiles, int64_t cells, int32_t* order,
-              int64_t* tile_start, void* workspace, cudaStream_t stream) {
-    if (n == 0) {
-        tile_starts_kernel<<<1, 256, 0, stream>>>(nullptr, 0, num_tiles, cells, tile_start);
-        count_launches(1);
-        return launch_status();
-    }
+// Sorts (key, value) pairs stably by key: the n keys (at most n_dev[0] of them when
+// n_dev is not null, a count known on the device only) with values vals_in (null: the
+// indices 0, 1, ...); the values in key order land in vals_out, the keys in keys_out
+// (null: a workspace buffer, returned). Keys are at most max_key; the passes take 8 to
+// 10 bits each, as few passes as 10-bit digits allow.
+static uint32_t* radix_sort(const uint32_t* keys, const int32_t* vals_in, int64_t n, const int64_t* n_dev,
+                            uint64_t max_key, int32_t* vals_out, uint32_t* keys_out, void* workspace, int& status,
+                            cudaStream_t stream) {
     const SortLayout L = sort_layout(n);
     char* ws = static_cast<char*>(workspace);
     uint32_t* ka = reinterpret_cast<uint32_t*>(ws + L.keys_a);
@@ -347,34 +349,270 @@ int sort_keys(const uint32_t* keys, int64_t n, int64_t num_tiles, int64_t cells,
     int32_t* vb = reinterpret_cast<int32_t*>(ws + L.vals_b);
     uint32_t* counts = reinterpret_cast<uint32_t*>(ws + L.counts);
     uint32_t* sums = reinterpret_cast<uint32_t*>(ws + L.sums);
-    const uint64_t max_key = (uint64_t)num_tiles * (uint64_t)cells;  // the sentinel
     int bits = 1;
     while (bits < 32 && (max_key >> bits) != 0) ++bits;
     const int passes = std::max(1, (bits + 9) / 10);
     const int digit_bits = std::max(8, (bits + passes - 1) / passes);
     const int64_t nb = sort_blocks(n);
     const uint32_t* kin = keys;
-    const int32_t* vin = nullptr;  // the first pass numbers the markers itself
+    const int32_t* vin = vals_in;
     uint32_t* kout_buf[2] = {ka, kb};
     int32_t* vout_buf[2] = {va, vb};
     uint32_t* kout = ka;
+    status = MPF_OK;
     for (int p = 0; p < passes; ++p) {
         const int shift = digit_bits * p;
-        kout = kout_buf[p & 1];
-        int32_t* vout = (p == passes - 1) ? order : vout_buf[p & 1];
-        int st;
-        if (digit_bits <= 8) st = radix_pass<8>(kin, vin, n, shift, counts, sums, nb, kout, vout, stream);
-        else if (digit_bits == 9) st = radix_pass<9>(kin, vin, n, shift, counts, sums, nb, kout, vout, stream);
-        else st = radix_pass<10>(kin, vin, n, shift, counts, sums, nb, kout, vout, stream);
-        if (st != MPF_OK) return st;
+        const bool last = p == passes - 1;
+        kout = (last && keys_out) ? keys_out : kout_buf[p & 1];
+        int32_t* vout = last ? vals_out : vout_buf[p & 1];
+        if (digit_bits <= 8) status = radix_pass<8>(kin, vin, n, n_dev, shift, counts, sums, nb, kout, vout, stream);
+        else if (digit_bits == 9) status = radix_pass<9>(kin, vin, n, n_dev, shift, counts, sums, nb, kout, vout, stream);
+        else status = radix_pass<10>(kin, vin, n, n_dev, shift, counts, sums, nb, kout, vout, stream);
+        if (status != MPF_OK) return kout;
         kin = kout;
         vin = vout;
     }
+    return kout;
+}
+
+static int tile_starts(const uint32_t* sorted, int64_t n, int64_t num_tiles, int64_t cells, int64_t* tile_start,
+                       cudaStream_t stream) {
     const int block = 256;
     const int64_t blocks = std::min<int64_t>((n + 1 + block - 1) / block, (int64_t)sm_count() * 16);
-    tile_starts_kernel<<<(unsigned)std::max<int64_t>(blocks, 1), block, 0, stream>>>(kout, n, num_tiles, cells, tile_start);
+    tile_starts_kernel<<<(unsigned)std::max<int64_t>(blocks, 1), block, 0, stream>>>(sorted, n, num_tiles, cells,
+                                                                                   tile_start);
     count_launches(1);
     return launch_status();
+}
+
+// Sort (keys, marker) pairs stably; the marker order lands in `order`, the tile starts
+// in `tile_start`; keys are at most num_tiles * cells (the sentinel).
+int sort_keys(const uint32_t* keys, int64_t n, int64_t num_tiles, int64_t cells, int32_t* order,
+              int64_t* tile_start, void* workspace, cudaStream_t stream) {
+    if (n == 0) return tile_starts(nullptr, 0, num_tiles, cells, tile_start, stream);
+    int st = MPF_OK;
+    const uint32_t* sorted = radix_sort(keys, nullptr, n, nullptr, (uint64_t)num_tiles * (uint64_t)cells, order,
+                                        nullptr, workspace, st, stream);
+    if (st != MPF_OK) return st;
+    return tile_starts(sorted, n, num_tiles, cells, tile_start, stream);
+}
+
+// ------------------------------------------------------ the incremental re-sort --
+//
+// A store sorted by key whose markers then moved a little: the new stable order is the
+// order of (new key, store rank). A marker whose key did not change (a stayer) keeps its
+// place among the other stayers -- their keys are the old ones, already ascending in
+// store order -- so only the markers whose key changed (the movers) need sorting. The
+// re-sort splits the ranks into stayers and movers (stable compaction), radix-sorts the
+// movers alone by (key, rank) (their count is known on the device only: the passes read
+// it there), and merges the two lists: the output rank of a stayer is its index among
+// the stayers plus the number of movers before it in (key, rank) order, found from the
+// first mover of every key and a binary search among the movers of its own key, and
+// likewise for a mover. The result is the order a full stable sort of the new keys gives,
+// bit for bit; its cost is a pass over the store plus a sort of the movers only.
+
+// Movers of every block of kSortTile ranks.
+__global__ void mover_count_kernel(const uint32_t* knew, const uint32_t* kprev, int64_t n, uint32_t* counts) {
+    __shared__ uint32_t part[kWarps];
+    const int64_t base = (int64_t)blockIdx.x * kSortTile;
+    uint32_t c = 0;
+    for (int k = threadIdx.x; k < kSortTile; k += blockDim.x) {
+        const int64_t i = base + k;
+        if (i < n && knew[i] != kprev[i]) ++c;
+    }
+    c = __reduce_add_sync(0xffffffffu, c);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 0;
+        for (int w = 0; w < kWarps; ++w) t += part[w];
+        counts[blockIdx.x] = t;
+    }
+}
+
+// Stable compaction of the ranks into stayers and movers (key and rank each), the block's
+// movers starting at offsets[block] (an exclusive scan of mover_count_kernel's counts).
+// The last block writes the totals: totals[0] movers, totals[1] stayers.
+__global__ void split_kernel(const uint32_t* knew, const uint32_t* kprev, int64_t n, const uint32_t* offsets,
+                             int64_t nblocks, uint32_t* s_keys, int32_t* s_ranks, uint32_t* m_keys,
+                             int32_t* m_ranks, int64_t* totals) {
+    __shared__ uint32_t warp_movers[kWarps];
+    __shared__ uint32_t carry;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t base = (int64_t)blockIdx.x * kSortTile;
+    if (threadIdx.x == 0) carry = 0;
+    const uint32_t first_mover = offsets[blockIdx.x];
+    __syncthreads();
+    for (int round = 0; round < kSortItems; ++round) {
+        const int64_t i = base + (int64_t)round * kSortBlock + threadIdx.x;
+        const bool have = i < n;
+        const uint32_t key = have ? knew[i] : 0;
+        const bool mover = have && key != kprev[i];
+        const unsigned ballot = __ballot_sync(0xffffffffu, mover);
+        if (lane == 0) warp_movers[warp] = __popc(ballot);
+        __syncthreads();
+        uint32_t before = carry;
+        for (int w = 0; w < warp; ++w) before += warp_movers[w];
+        before += __popc(ballot & ((1u << lane) - 1u));  // movers of this round before this rank
+        if (have) {
+            const int64_t movers_before = (int64_t)first_mover + before;
+            if (mover) {
+                m_keys[movers_before] = key;
+                m_ranks[movers_before] = (int32_t)i;
+            } else {
+                const int64_t stayers_before = i - movers_before;
+                s_keys[stayers_before] = key;
+                s_ranks[stayers_before] = (int32_t)i;
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t t = 0;
+            for (int w = 0; w < kWarps; ++w) t += warp_movers[w];
+            carry += t;
+        }
+        __syncthreads();
+    }
+    if (blockIdx.x == nblocks - 1 && threadIdx.x == 0) {
+        totals[0] = (int64_t)first_mover + carry;
+        totals[1] = n - totals[0];
+    }
+}
+
+// starts[k] = the first index of a sorted key array at or above key k, k = 0 .. nkeys;
+// the array holds *count keys (count known on the device).
+__global__ void key_starts_kernel(const uint32_t* sorted, int64_t n_max, const int64_t* count, int64_t nkeys,
+                                  int32_t* starts) {
+    const int64_t n = min(n_max, *count);
+    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j <= n;
+         j += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t prev = j == 0 ? -1 : (int64_t)sorted[j - 1];
+        const int64_t cur = j == n ? nkeys : min((int64_t)sorted[j], nkeys);
+        for (int64_t k = prev + 1; k <= cur; ++k) starts[k] = (int32_t)j;
+    }
+}
+
+// The number of ranks[lo .. hi) below r (ranks ascending).
+__device__ __forceinline__ int32_t ranks_below(const int32_t* ranks, int32_t lo, int32_t hi, int32_t r) {
+    while (lo < hi) {
+        const int32_t mid = lo + (hi - lo) / 2;
+        if (ranks[mid] < r) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// The merge: every stayer and every mover to its output rank; order[rank] = its store
+// rank, keys_out[rank] = its key.
+__global__ void merge_place_kernel(const uint32_t* s_keys, const int32_t* s_ranks, const int32_t* s_starts,
+                                   const uint32_t* m_keys, const int32_t* m_ranks, const int32_t* m_starts,
+                                   const int64_t* totals, int64_t n, int64_t nkeys, int32_t* order,
+                                   uint32_t* keys_out) {
+    const int64_t movers = totals[0], stayers = totals[1];
+    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
+        const bool stayer = j < stayers;
+        const int64_t idx = stayer ? j : j - stayers;
+        if (!stayer && idx >= movers) continue;
+        const uint32_t key = stayer ? s_keys[idx] : m_keys[idx];
+        const int32_t rank = stayer ? s_ranks[idx] : m_ranks[idx];
+        const int64_t k = min((int64_t)key, nkeys - 1);
+        // the other list's elements before this one: all of smaller keys, and those of the
+        // same key with smaller store ranks
+        const int32_t* other_starts = stayer ? m_starts : s_starts;
+        const int32_t* other_ranks = stayer ? m_ranks : s_ranks;
+        const int32_t before = ranks_below(other_ranks, other_starts[k], other_starts[k + 1], rank);
+        const int64_t at = idx + before;
+        if (at >= 0 && at < n) {
+            order[at] = rank;
+            keys_out[at] = key;
+        }
+    }
+}
+
+struct ResortLayout {
+    size_t keys_new, s_keys, s_ranks, m_keys, m_ranks, m_sorted_keys, m_sorted_ranks, counts, sums, totals,
+        s_starts, m_starts, radix, total;
+};
+
+static ResortLayout resort_layout(int64_t n, int64_t nkeys) {
+    const size_t items = align256(sizeof(uint32_t) * (size_t)(n > 0 ? n : 1));
+    const int64_t nb = sort_blocks(n);
+    const size_t starts = align256(sizeof(int32_t) * (size_t)(nkeys + 1));
+    ResortLayout L{};
+    size_t off = 0;
+    L.keys_new = off; off += items;
+    L.s_keys = off; off += items;
+    L.s_ranks = off; off += items;
+    L.m_keys = off; off += items;
+    L.m_ranks = off; off += items;
+    L.m_sorted_keys = off; off += items;
+    L.m_sorted_ranks = off; off += items;
+    L.counts = off; off += align256(sizeof(uint32_t) * (size_t)nb);
+    L.sums = off; off += align256(sizeof(uint32_t) * (size_t)scan_chunks(nb));
+    L.totals = off; off += 256;
+    L.s_starts = off; off += starts;
+    L.m_starts = off; off += starts;
+    L.radix = off; off += sort_layout(n).total;
+    L.total = off;
+    return L;
+}
+
+size_t resort_workspace_bytes(int64_t n, int64_t nkeys) { return resort_layout(n, nkeys).total; }
+
+// The keys of the store's markers are in the workspace (resort_keys_buffer); with
+// prev_sorted null a full sort, else the re-sort against the store's previous sorted keys.
+uint32_t* resort_keys_buffer(void* workspace, int64_t n) {
+    return reinterpret_cast<uint32_t*>(static_cast<char*>(workspace) + resort_layout(n, 1).keys_new);
+}
+
+int resort_keys(int64_t n, int64_t num_tiles, int64_t cells, const uint32_t* prev_sorted, uint32_t* sorted_out,
+                int32_t* order, int64_t* tile_start, void* workspace, cudaStream_t stream) {
+    const int64_t nkeys = num_tiles * cells + 1;  // keys 0 .. the sentinel
+    const ResortLayout L = resort_layout(n, nkeys);
+    char* ws = static_cast<char*>(workspace);
+    auto at = [&](size_t off) { return reinterpret_cast<void*>(ws + off); };
+    const uint32_t* knew = static_cast<const uint32_t*>(at(L.keys_new));
+    if (n == 0) return tile_starts(nullptr, 0, num_tiles, cells, tile_start, stream);
+    const uint64_t max_key = (uint64_t)num_tiles * (uint64_t)cells;
+    int st = MPF_OK;
+    if (!prev_sorted) {
+        radix_sort(knew, nullptr, n, nullptr, max_key, order, sorted_out, at(L.radix), st, stream);
+        if (st != MPF_OK) return st;
+        return tile_starts(sorted_out, n, num_tiles, cells, tile_start, stream);
+    }
+    uint32_t* counts = static_cast<uint32_t*>(at(L.counts));
+    uint32_t* sums = static_cast<uint32_t*>(at(L.sums));
+    int64_t* totals = static_cast<int64_t*>(at(L.totals));
+    uint32_t* s_keys = static_cast<uint32_t*>(at(L.s_keys));
+    int32_t* s_ranks = static_cast<int32_t*>(at(L.s_ranks));
+    uint32_t* m_keys = static_cast<uint32_t*>(at(L.m_keys));
+    int32_t* m_ranks = static_cast<int32_t*>(at(L.m_ranks));
+    uint32_t* m_sorted_keys = static_cast<uint32_t*>(at(L.m_sorted_keys));
+    int32_t* m_sorted_ranks = static_cast<int32_t*>(at(L.m_sorted_ranks));
+    int32_t* s_starts = static_cast<int32_t*>(at(L.s_starts));
+    int32_t* m_starts = static_cast<int32_t*>(at(L.m_starts));
+    const int64_t nb = sort_blocks(n);
+    mover_count_kernel<<<(unsigned)nb, kSortBlock, 0, stream>>>(knew, prev_sorted, n, counts);
+    count_launches(1);
+    if ((st = launch_status()) != MPF_OK) return st;
+    if ((st = scan_exclusive(counts, nb, sums, stream)) != MPF_OK) return st;
+    split_kernel<<<(unsigned)nb, kSortBlock, 0, stream>>>(knew, prev_sorted, n, counts, nb, s_keys, s_ranks, m_keys,
+                                                          m_ranks, totals);
+    count_launches(1);
+    if ((st = launch_status()) != MPF_OK) return st;
+    // the movers by (key, rank): a stable sort of their keys carrying their ranks
+    radix_sort(m_keys, m_ranks, n, totals, max_key, m_sorted_ranks, m_sorted_keys, at(L.radix), st, stream);
+    if (st != MPF_OK) return st;
+    const int block = 256;
+    const int64_t blocks = std::min<int64_t>((n + 1 + block - 1) / block, (int64_t)sm_count() * 16);
+    key_starts_kernel<<<(unsigned)blocks, block, 0, stream>>>(s_keys, n, totals + 1, nkeys, s_starts);
+    key_starts_kernel<<<(unsigned)blocks, block, 0, stream>>>(m_sorted_keys, n, totals, nkeys, m_starts);
+    merge_place_kernel<<<(unsigned)blocks, block, 0, stream>>>(s_keys, s_ranks, s_starts, m_sorted_keys,
+                                                              m_sorted_ranks, m_starts, totals, n, nkeys, order,
+                                                              sorted_out);
+    count_launches(3);
+    if ((st = launch_status()) != MPF_OK) return st;
+    return tile_starts(sorted_out, n, num_tiles, cells, tile_start, stream);
 }
 
 int permute_rows(void* dst, int64_t ds, const void* src, int64_t ss, int64_t rows, const int32_t* order,

@@ -25,13 +25,14 @@ from mpifield_b200.kernels import _marker_rows
 
 @dataclass
 class TileOrder:
-    """The result of `sort_by_tile`."""
+    """The result of `sort_by_tile` and `resort_by_tile`."""
 
-    keys: torch.Tensor        # (N,) int32 view of the uint32 keys, in marker order
-    order: torch.Tensor       # (N,) int32: the marker of every rank
-    tile_start: torch.Tensor  # (num_tiles + 2,) int64: first rank of every key, then N
+    keys: torch.Tensor | None  # (N,) int32 view of the uint32 keys, in marker order (sort_by_tile)
+    order: torch.Tensor        # (N,) int32: the marker of every rank
+    tile_start: torch.Tensor   # (num_tiles + 2,) int64: first rank of every tile, then N
     num_tiles: int
-    tile: tuple = ()          # anchor nodes per tile, per axis
+    tile: tuple = ()           # anchor nodes per tile, per axis
+    sorted_keys: torch.Tensor | None = None  # (N,) int32 view of the keys in rank order (resort_by_tile)
 
 
 def _kind_of(weighting) -> tuple[int, int]:
@@ -105,6 +106,54 @@ def sort_by_tile(positions: torch.Tensor, weighting, geometry, tile, values: tor
         _lib.F64 if p.dtype == "f8" else _lib.F32, stream)
     _lib.check(status, "sort_by_tile")
     return TileOrder(keys, order, tile_start, ntiles, tuple(int(v) for v in tile))
+
+
+def resort_by_tile(positions, weighting, geometry, tile, values=None, within: bool = False,
+                   previous: TileOrder | None = None, alloc=None) -> TileOrder:
+    """Sort a marker store by cell tile, again: ``positions`` (and ``values``) are the store's
+    arrays in their current order, ``previous`` the `TileOrder` this function returned for
+    the store before its markers moved (after which the store's arrays were permuted by its
+    ``order``), or None for the first sort. The result is the order `sort_by_tile` gives,
+    bit for bit, with ``sorted_keys`` for the next call; with ``previous`` only the markers
+    whose key changed are sorted (mpf_resort_by_tile). ``alloc`` as in `sort_by_tile`.
+    """
+    kind, degree = _kind_of(weighting)
+    lower, cell, num, code, ndim = _lib.geometry_arrays(geometry)
+    p = as_device_array(positions, "positions")
+    v = None if values is None else as_device_array(values, "values")
+    stream = launch_stream(*(a for a in (p, v) if a is not None))
+    if p.dtype not in ("f8", "f4"):
+        raise TypeError(f"positions must be float64 or float32, got {p.dtype}")
+    pos, ps = _marker_rows(p, ndim, "positions", p.dtype, stream)
+    n = pos.shape[1]
+    ntiles = num_tiles((kind, degree), geometry, tile)
+    t = (C.c_int32 * ndim)(*(int(x) for x in tile))
+    if previous is not None:
+        if previous.sorted_keys is None or previous.sorted_keys.numel() != n or tuple(previous.tile) != tuple(
+                int(x) for x in tile):
+            raise ValueError("previous must be the resort_by_tile result of this store (same markers and tile)")
+    size = C.c_size_t(0)
+    _lib.check(_lib.library().mpf_resort_workspace_bytes(kind, degree, ndim, num, code, t, int(bool(within)), n,
+                                                       C.byref(size)), "resort_workspace_bytes")
+    device = pos.torch().device
+    new = alloc or (lambda shape, dt: _empty(shape, dt, device))
+    with torch_on(stream):
+        workspace = new((max(int(size.value), 256),), torch.uint8)
+        order = new((n,), torch.int32)
+        sorted_keys = new((n,), torch.int32)
+        tile_start = new((ntiles + 2,), torch.int64)
+    if v is not None:
+        vals, vs = _marker_rows(v, v.shape[0] if v.ndim == 2 else 1, "values", p.dtype, stream)
+        vptr, ncomp = vals.ptr, vals.shape[0]
+    else:
+        vptr, vs, ncomp = None, 0, 0
+    prev = previous.sorted_keys.data_ptr() if previous is not None else None
+    status = _lib.library().mpf_resort_by_tile(
+        kind, degree, ndim, pos.ptr, ps, vptr, vs, ncomp, n, lower, cell, num, code, t, int(bool(within)), prev,
+        sorted_keys.data_ptr(), order.data_ptr(), tile_start.data_ptr(), workspace.data_ptr(), workspace.numel(),
+        _lib.F64 if p.dtype == "f8" else _lib.F32, stream)
+    _lib.check(status, "resort_by_tile")
+    return TileOrder(None, order, tile_start, ntiles, tuple(int(x) for x in tile), sorted_keys)
 
 
 def permute(array: torch.Tensor, order: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:

@@ -88,6 +88,14 @@ def test_invalid_arguments_return_a_status_before_any_device_work():
                                          16, None) == _lib.ERR_WORKSPACE
     assert lib.mpf_scatter_deterministic(1, 2, 3, fake, 0, fake, 0, 10, fake, 1, lower, cell, num, code, fake + 8,
                                          size.value, None) == _lib.ERR_ALIGNMENT
+    # the re-sort: a workspace too small, the previous keys given as the output
+    t3 = (C.c_int32 * 3)(4, 4, 4)
+    size = C.c_size_t()
+    assert lib.mpf_resort_workspace_bytes(1, 2, 3, num, code, t3, 1, 1000, C.byref(size)) == 0
+    assert lib.mpf_resort_by_tile(1, 2, 3, fake, 0, None, 0, 0, 1000, lower, cell, num, code, t3, 1, None, fake, fake,
+                                  fake, fake, 16, 0, None) == _lib.ERR_WORKSPACE
+    assert lib.mpf_resort_by_tile(1, 2, 3, fake, 0, None, 0, 0, 1000, lower, cell, num, code, t3, 1, fake, fake, fake,
+                                  fake, fake, size.value, 0, None) == _lib.ERR_ARGUMENT
     # a workspace too small
     t = (C.c_int32 * 3)(4, 4, 4)
     assert lib.mpf_sort_by_tile(1, 2, 3, fake, 0, None, 0, 0, 1000, lower, cell, num, code, t, 0, fake, fake, fake,
