@@ -575,6 +575,7 @@ def run_ours(args, world, rank, local) -> None:
         torch.cuda.empty_cache()
         extras["autograd"] = measure_autograd(device, reps, peak)
         extras["path_deposit"] = measure_paths(device, reps, peak)
+        extras["forms_and_clamped"] = measure_forms_and_clamped(device, reps)
         if args.serve_requests > 0:
             from mpifield_b200 import serving
 
@@ -793,6 +794,55 @@ def measure_autograd(device, reps: int, peak: float) -> dict:
         out[name] = {"value": n / (ms / 1000.0), "ms_per_step": ms, "best_ms": best,
                      "algorithmic_bytes": nbytes, "hbm_frac": nbytes / (ms / 1000.0) / 1e9 / peak}
     out["reference"] = "none: the reference has no differentiation"
+    return out
+
+
+def measure_forms_and_clamped(device, reps: int) -> dict:
+    """The k-form kernels and clamped axes: 3D, 128^3 nodes on the unit cube, N = 2^24
+    uniform markers (random order). Faces (2-forms, 3 components) and cells (top form)
+    of degree 2, gather + scatter, periodic; then CUBIC node gather (3 components) +
+    scatter with every axis clamped (Cox-de Boor knots) beside the same on periodic
+    axes."""
+    import mpifield_b200 as mf
+    from mpifield_b200.kernels import gather, gather_forms, scatter, scatter_forms
+
+    n, g_n = 1 << 24, 128
+    g = torch.Generator(device=device).manual_seed(12)
+    pos = torch.rand((3, n), generator=g, device=device, dtype=torch.float64)
+    vals3 = torch.rand((3, n), generator=g, device=device, dtype=torch.float64) + 0.5
+    out = {"config": f"{g_n}^3 on the unit cube, N={n} uniform markers in random order", "unit": "markers/s"}
+    h = 1.0 / g_n
+    periodic = (0.0, 0.0, 0.0, h, h, h, g_n, g_n, g_n, 1, 1, 1)
+    res3 = torch.empty((3, n), dtype=torch.float64, device=device)
+    for form, name, nc in ((2, "faces_quadratic", 3), (3, "cells_quadratic", 1)):
+        field = torch.rand((g_n, g_n, g_n, nc), generator=g, device=device, dtype=torch.float64)
+        dep = torch.zeros_like(field)
+
+        def go():
+            gather_forms(2, form, pos, field, res3[:nc], periodic)
+            dep.zero_()
+            scatter_forms(2, form, pos, vals3[:nc], dep, periodic)
+
+        ms, best = _event_stats(go, reps)
+        out[name] = {"value": n / (ms / 1000.0), "ms": ms, "best_ms": best}
+        del field, dep
+    hc = 1.0 / (g_n - 1)
+    clamped = (0.0, 0.0, 0.0, hc, hc, hc, g_n, g_n, g_n, 2, 2, 2)
+    for codes, geom, name in (("clamped", clamped, "cubic_clamped"), ("periodic", periodic, "cubic_periodic")):
+        ext = g_n + 2 if codes == "clamped" else g_n
+        field = torch.rand((ext, ext, ext, 3), generator=g, device=device, dtype=torch.float64)
+        dens = torch.zeros((ext, ext, ext, 1), dtype=torch.float64, device=device)
+
+        def go():
+            gather(mf.kernels._lib.SPLINE, 3, pos, field, res3, geom)
+            dens.zero_()
+            scatter(mf.kernels._lib.SPLINE, 3, pos, vals3[:1], dens, geom)
+
+        ms, best = _event_stats(go, reps)
+        out[name] = {"value": n / (ms / 1000.0), "ms": ms, "best_ms": best}
+        del field, dens
+    del pos, vals3, res3
+    torch.cuda.empty_cache()
     return out
 
 

@@ -282,6 +282,28 @@ MPF_API int mpf_sort_by_tile(int kind, int degree, int ndim, const void* positio
                      int dtype, void* stream);
 
 /*
+ * k-forms of B-spline degree 1-3 (form 1 .. ndim): component c of a `form`-form weighs
+ * the degree-`degree` B-spline along the axes it is not staggered on and the edge
+ * functions B_(degree-1)(r - k - 1/2) (existing edges only) along those it is -- an edge
+ * (form 1) along its direction, a face of 3D (form 2) across its normal, the top form
+ * (form ndim) along every axis; positions are clamped on bounded and clamped axes. The
+ * field is extent + (ncomp,) with ncomp = ndim choose form (extent num + degree - 1 on a
+ * clamped axis). mpf_gather_forms overwrites result (ncomp, n); mpf_scatter_forms adds
+ * values (ncomp, n) into the field, skipping markers whose values are all zero before
+ * reading their positions. Replace gather_forms_spline_{1,2,3}d and
+ * scatter_forms_spline_{1,2,3}d (src/mpifield/kernels/spline_forms.py:85-138, used by
+ * the faces and cells of src/mpifield/splines.py:185-205).
+ */
+MPF_API int mpf_gather_forms(int degree, int form, int ndim, const void* positions, int64_t pos_stride, int64_t n,
+                             const void* field, int64_t ncomp, void* result, int64_t res_stride,
+                             const double* lower, const double* cell, const int32_t* num, const int32_t* code,
+                             int dtype, void* stream);
+MPF_API int mpf_scatter_forms(int degree, int form, int ndim, const void* positions, int64_t pos_stride,
+                              const void* values, int64_t val_stride, int64_t n, void* field, int64_t ncomp,
+                              const double* lower, const double* cell, const int32_t* num,
+                              const int32_t* code, int dtype, void* stream);
+
+/*
  * The cell-tile sort of a store that is kept sorted: the markers' keys as in
  * mpf_sort_by_tile, computed from the positions (and values) in the store's current
  * order; order[j] is the current rank of the marker of new rank j in the stable

@@ -86,6 +86,8 @@ _SIGNATURES = {
                           C.c_size_t, _I, _P], _I),
     "mpf_sort_by_tile_noalloc": ([_I, _I, _I, _P, _L, _P, _L, _L, _L, _P, _P, _P, _P, _P, _I, _P, _P, _P, _I,
                                   _P], _I),
+    "mpf_gather_forms": ([_I, _I, _I, _P, _L, _L, _P, _L, _P, _L, _P, _P, _P, _P, _I, _P], _I),
+    "mpf_scatter_forms": ([_I, _I, _I, _P, _L, _P, _L, _L, _P, _L, _P, _P, _P, _P, _I, _P], _I),
     "mpf_resort_workspace_bytes": ([_I, _I, _I, _P, _P, _P, _I, _L, _P], _I),
     "mpf_resort_by_tile": ([_I, _I, _I, _P, _L, _P, _L, _L, _L, _P, _P, _P, _P, _P, _I, _P, _P, _P, _P, _P,
                             C.c_size_t, _I, _P], _I),

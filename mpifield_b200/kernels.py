@@ -416,6 +416,76 @@ def gather_edges(kind: int, degree: int, positions, edges, result, geometry) -> 
     out.finish()
 
 
+def form_components(form: int, ndim: int) -> int:
+    """The components of a ``form``-form in ``ndim`` dimensions: ndim choose form."""
+    return {(1, 1): 1, (1, 2): 2, (2, 2): 1, (1, 3): 3, (2, 3): 3, (3, 3): 1}[(form, ndim)]
+
+
+def gather_forms(degree: int, form: int, positions, field, result, geometry) -> None:
+    """result(c, i) = the ``form``-form ``field`` (extent + (ncomp,)) at marker i, component c."""
+    lower, cell, num, code, ndim = _lib.geometry_arrays(geometry)
+    a, stream = _arrays(positions=positions, field=field, result=result)
+    dtype = a["field"].dtype
+    f = _field(a["field"], _extent(num, code, degree), "field")
+    if not f.is_contiguous():
+        f = _copied(f, f.shape, dtype, stream)
+    ncomp = f.shape[-1]
+    pos, ps = _marker_rows(a["positions"], ndim, "positions", dtype, stream)
+    n = pos.shape[1]
+    if a["result"].shape != (ncomp, n) and not (ncomp == 1 and a["result"].shape == (n,)):
+        raise ValueError(f"result must be ({ncomp}, {n}), got {a['result'].shape}")
+    res = a["result"]
+    if res.ndim == 1:
+        res = DeviceArray(res.ptr, (1, n), (n, res.strides[0]), res.dtype, res.source, res.stream, res.device)
+    out = _Output(res, dtype, accumulate=False, stream=stream, rows=ncomp)
+    status = _lib.library().mpf_gather_forms(degree, form, ndim, pos.ptr, ps, n, f.ptr, ncomp, out.work.ptr,
+                                              out.row_stride, lower, cell, num, code, _dtype_code(f, "field"), stream)
+    _lib.check(status, "gather_forms")
+    out.finish()
+
+
+def scatter_forms(degree: int, form: int, positions, values, field, geometry) -> None:
+    """field(k, c) += the ``form``-form weights of markers' ``values`` (ncomp, N)."""
+    lower, cell, num, code, ndim = _lib.geometry_arrays(geometry)
+    a, stream = _arrays(positions=positions, values=values, field=field)
+    dtype = a["field"].dtype
+    f = _field(a["field"], _extent(num, code, degree), "field")
+    ncomp = f.shape[-1]
+    pos, ps = _marker_rows(a["positions"], ndim, "positions", dtype, stream)
+    vals, vs = _marker_rows(a["values"], ncomp, "values", dtype, stream)
+    if vals.shape[1] != pos.shape[1]:
+        raise ValueError(f"{pos.shape[1]} positions and {vals.shape[1]} values")
+    out = _Output(f, dtype, accumulate=True, stream=stream)
+    status = _lib.library().mpf_scatter_forms(degree, form, ndim, pos.ptr, ps, vals.ptr, vs, pos.shape[1],
+                                               out.work.ptr, ncomp, lower, cell, num, code, _dtype_code(f, "field"),
+                                               stream)
+    _lib.check(status, "scatter_forms")
+    out.finish()
+
+
+@dataclass(frozen=True)
+class FormKernel:
+    """A k-form gather or scatter: gather_forms_spline_{n}d / scatter_forms_spline_{n}d with
+    ``degree`` and ``form`` as the last two arguments, or fixed (``fixed``: (degree, form))."""
+
+    op: str
+    ndim: int
+    fixed: tuple | None = None
+
+    def __call__(self, *args, **launch) -> None:
+        if self.fixed is None:
+            *args, degree, form = args
+        else:
+            degree, form = self.fixed
+        with _launch_options(f"{self.op} forms kernel", launch):
+            if self.op == "gather":
+                positions, field, result, *geometry = args
+                gather_forms(int(degree), int(form), positions, field, result, geometry)
+            else:
+                positions, values, field, *geometry = args
+                scatter_forms(int(degree), int(form), positions, values, field, geometry)
+
+
 def _catalog() -> dict:
     kernels = {}
     for n in (1, 2, 3):
@@ -429,6 +499,8 @@ def _catalog() -> dict:
         kernels[f"deposit_paths_spline_{n}d"] = PathKernel(_lib.SPLINE, n, True)
         kernels[f"gather_edges_{n}d"] = EdgeGatherKernel(_lib.LINEAR, n, False)
         kernels[f"gather_edges_spline_{n}d"] = EdgeGatherKernel(_lib.SPLINE, n, True)
+        kernels[f"gather_forms_spline_{n}d"] = FormKernel("gather", n)
+        kernels[f"scatter_forms_spline_{n}d"] = FormKernel("scatter", n)
     return kernels
 
 

@@ -1,11 +1,12 @@
-"""The B-spline families: the node and edge weightings of one degree, paired.
+"""The B-spline families: the weightings of every form of one degree.
 
 mpifield's ``Splines`` (src/mpifield/splines.py:100-272) names, for a degree, the
 weighting of every form: ``nodes`` (0-forms), ``edges`` (1-forms), ``faces`` (2-forms,
-3D) and ``cells`` (top forms). This backend covers the node and edge weightings of
-degrees 1-3 with its own kernels; `faces` and `cells` stay None here. `SPLINES` holds
-the built-in families; `CLAMPED_SPLINES` those whose weightings all take clamped axes
-(every one on the spline kernels), and `splines` picks one.
+3D) and ``cells`` (top forms, 1D to 3D), all on this backend's kernels; the faces and
+cells run the k-form kernels (`kernels.FormKernel`, mpf_gather_forms / mpf_scatter_forms)
+and take clamped axes. `SPLINES` holds the built-in families; `CLAMPED_SPLINES` those
+whose weightings all take clamped axes (every one on the spline kernels), and `splines`
+picks one.
 """
 
 from __future__ import annotations
@@ -13,6 +14,7 @@ from __future__ import annotations
 from dataclasses import dataclass
 
 from mpifield_b200.edges import CUBIC_EDGES, QUADRATIC_EDGES, WHITNEY, EdgeWeighting, spline_edges
+from mpifield_b200.kernels import FormKernel
 from mpifield_b200.weighting import CUBIC, LINEAR, QUADRATIC, Weighting, spline_weighting
 
 __all__ = ["CLAMPED_SPLINES", "SPLINES", "Splines", "splines"]
@@ -63,18 +65,40 @@ class Splines:
         return f"Splines(degree {self.degree}: {names}{', clamped' if self.clamped else ''})"
 
 
+_NAMES = {1: "linear", 2: "quadratic", 3: "cubic"}
+
+
+def _faces(degree: int) -> Weighting:
+    """The 2-forms of a degree in 3D: one component per face normal."""
+    fixed = (degree, 2)
+    return Weighting(f"{_NAMES[degree]} faces", scatter={3: FormKernel("scatter", 3, fixed)},
+                     gather={3: FormKernel("gather", 3, fixed)}, halo=2 if degree > 1 else 1, clamps=True)
+
+
+def _cells(degree: int) -> Weighting:
+    """The top forms of a degree in 1D to 3D: one component."""
+    return Weighting(f"{_NAMES[degree]} cells",
+                     scatter={n: FormKernel("scatter", n, (degree, n)) for n in (1, 2, 3)},
+                     gather={n: FormKernel("gather", n, (degree, n)) for n in (1, 2, 3)},
+                     halo=2 if degree > 1 else 1, clamps=True)
+
+
+_FACES = {d: _faces(d) for d in (1, 2, 3)}
+_CELLS = {d: _cells(d) for d in (1, 2, 3)}
+
+
 def _family(degree: int, clamped: bool) -> Splines:
     if not clamped:
         nodes = {1: LINEAR, 2: QUADRATIC, 3: CUBIC}[degree]
         edges = {1: WHITNEY, 2: QUADRATIC_EDGES, 3: CUBIC_EDGES}[degree]
-        return Splines(degree, nodes, edges)
+        return Splines(degree, nodes, edges, _FACES[degree], _CELLS[degree])
     # on clamped axes every weighting runs on the spline kernels (degree 3 already does)
     name = {1: "linear", 2: "quadratic", 3: "cubic"}[degree]
     nodes = CUBIC if degree == 3 else spline_weighting(degree, name)
     nodes = Weighting(nodes.name, nodes.scatter, nodes.gather, halo=2 if degree > 1 else 1, degree=degree,
                       clamps=True)
     edges = {1: spline_edges("linear", 1), 2: QUADRATIC_EDGES, 3: CUBIC_EDGES}[degree]
-    return Splines(degree, nodes, edges, clamped=True)
+    return Splines(degree, nodes, edges, _FACES[degree], _CELLS[degree], clamped=True)
 
 
 #: The built-in families, by degree.

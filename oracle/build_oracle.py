@@ -39,7 +39,8 @@ REF_CUDA_SO = REF_OUT / "libref_cuda.so"
 REFERENCE_SRC = Path(os.environ.get("MPF_REFERENCE_SRC", Path(__file__).resolve().parents[2] / "reference" / "src"))
 KERNELS = REFERENCE_SRC / "mpifield" / "kernels"
 
-#: The reference kernels compiled into the _ref libraries: the hot path and the edge gathers.
+#: The reference kernels compiled into the _ref libraries: the hot path, the edge gathers and
+#: the k-form kernels.
 REF_KERNELS = [
     f"{op}_{kind}_{n}d"
     for op in ("gather", "scatter")
@@ -47,7 +48,8 @@ REF_KERNELS = [
     for n in (1, 2, 3)
 ] + [
     f"{name}_{n}d"
-    for name in ("deposit_paths", "deposit_paths_spline", "gather_edges", "gather_edges_spline")
+    for name in ("deposit_paths", "deposit_paths_spline", "gather_edges", "gather_edges_spline",
+                 "gather_forms_spline", "scatter_forms_spline")
     for n in (1, 2, 3)
 ]
 

@@ -783,6 +783,122 @@ void og_gather_edges(int ndim, int degree, const double* pos, int64_t pos_stride
     }
 }
 
+/* ------------------------------------------------------------- k-forms --- */
+
+/* Whether component `component` of a `form`-form in `ndim` dimensions is staggered along
+ * `axis` (spline_forms.py:30-40): the top form along every axis, the edges (1-forms) along
+ * their direction, the faces of 3D (2-forms) across their normal. */
+static int og_staggered(int form, int ndim, int component, int axis) {
+    if (form == ndim) return 1;
+    if (form == 1) return axis == component;
+    if (form == 2 && ndim == 3) return axis != component;
+    return 0;
+}
+
+/* The stencil of a k-form component at the clamped position rel (spline_forms.py:56-75):
+ * the B_(p-1) edges along the staggered axes (with their existence), the B_p nodes along
+ * the others; cnt[d] entries per axis. */
+static void og_form_stencil(const double* rel, const int32_t* num, const int32_t* code, int ndim, int degree,
+                            int form, int component, int idx[3][4], double wt[3][4], int ex[3][4], int cnt[3]) {
+    for (int d = 0; d < 3; ++d) {
+        idx[d][0] = 0;
+        wt[d][0] = 1.0;
+        ex[d][0] = 1;
+        cnt[d] = 1;
+    }
+    for (int d = 0; d < ndim; ++d) {
+        if (og_staggered(form, ndim, component, d)) {
+            og_along_stencil(rel[d], num[d], code[d], degree, idx[d], wt[d], ex[d]);
+            cnt[d] = degree;
+        } else {
+            og_axis s;
+            og_spline_cell(rel[d], num[d], code[d], degree, &s);
+            for (int a = 0; a <= degree; ++a) {
+                idx[d][a] = s.node[a];
+                wt[d][a] = s.w[a];
+                ex[d][a] = 1;
+            }
+            cnt[d] = degree + 1;
+        }
+    }
+}
+
+static void og_form_positions(int ndim, const double* pos, int64_t pos_stride, int64_t i, const double* lower,
+                              const double* cell, const int32_t* num, const int32_t* code, double* rel) {
+    for (int d = 0; d < ndim; ++d) {
+        rel[d] = (pos[d * pos_stride + i] - lower[d]) / cell[d];
+        if (code[d] != 1) {
+            const double top = (double)(num[d] - 1);
+            if (rel[d] < 0.0) rel[d] = 0.0;
+            if (rel[d] > top) rel[d] = top;
+        }
+    }
+}
+
+/* The gather of a k-form of degree 1..3 (gather_forms_spline, spline_forms.py:85-108):
+ * result(c, i) = sum over the stencil of component c of W field(k, c). The field is
+ * extent + (ncomp,), the extent num + degree - 1 along a clamped axis. */
+void og_gather_forms(int ndim, int degree, int form, const double* pos, int64_t pos_stride, int64_t n,
+                     const double* field, int64_t ncomp, double* result, int64_t res_stride, const double* lower,
+                     const double* cell, const int32_t* num, const int32_t* code) {
+    int ext[3] = {1, 1, 1};
+    for (int d = 0; d < ndim; ++d) ext[d] = og_extent(num[d], code[d], degree);
+    for (int64_t i = 0; i < n; ++i) {
+        double rel[3] = {0.0, 0.0, 0.0};
+        og_form_positions(ndim, pos, pos_stride, i, lower, cell, num, code, rel);
+        for (int c = 0; c < ncomp; ++c) {
+            int idx[3][4], ex[3][4], cnt[3];
+            double wt[3][4];
+            og_form_stencil(rel, num, code, ndim, degree, form, c, idx, wt, ex, cnt);
+            double total = 0.0;
+            for (int a = 0; a < cnt[0]; ++a)
+                for (int b = 0; b < cnt[1]; ++b)
+                    for (int e = 0; e < cnt[2]; ++e) {
+                        if (!(ex[0][a] && ex[1][b] && ex[2][e])) continue;
+                        double w = wt[0][a];
+                        if (ndim > 1) w = w * wt[1][b];
+                        if (ndim > 2) w = w * wt[2][e];
+                        const int64_t node = ((int64_t)idx[0][a] * ext[1] + idx[1][b]) * ext[2] + idx[2][e];
+                        total += w * field[node * ncomp + c];
+                    }
+            result[c * res_stride + i] = total;
+        }
+    }
+}
+
+/* The scatter of a k-form (scatter_forms_spline, spline_forms.py:111-138): field(k, c) +=
+ * W values(c, i); a marker whose values are all zero is skipped before its position is
+ * read. */
+void og_scatter_forms(int ndim, int degree, int form, const double* pos, int64_t pos_stride, const double* values,
+                      int64_t val_stride, int64_t n, double* field, int64_t ncomp, const double* lower,
+                      const double* cell, const int32_t* num, const int32_t* code) {
+    int ext[3] = {1, 1, 1};
+    for (int d = 0; d < ndim; ++d) ext[d] = og_extent(num[d], code[d], degree);
+    for (int64_t i = 0; i < n; ++i) {
+        int live = 0;
+        for (int c = 0; c < ncomp; ++c) live = live || values[c * val_stride + i] != 0.0;
+        if (!live) continue;
+        double rel[3] = {0.0, 0.0, 0.0};
+        og_form_positions(ndim, pos, pos_stride, i, lower, cell, num, code, rel);
+        for (int c = 0; c < ncomp; ++c) {
+            int idx[3][4], ex[3][4], cnt[3];
+            double wt[3][4];
+            og_form_stencil(rel, num, code, ndim, degree, form, c, idx, wt, ex, cnt);
+            const double v = values[c * val_stride + i];
+            for (int a = 0; a < cnt[0]; ++a)
+                for (int b = 0; b < cnt[1]; ++b)
+                    for (int e = 0; e < cnt[2]; ++e) {
+                        if (!(ex[0][a] && ex[1][b] && ex[2][e])) continue;
+                        double w = wt[0][a];
+                        if (ndim > 1) w = w * wt[1][b];
+                        if (ndim > 2) w = w * wt[2][e];
+                        const int64_t node = ((int64_t)idx[0][a] * ext[1] + idx[1][b]) * ext[2] + idx[2][e];
+                        field[node * ncomp + c] += w * v;
+                    }
+        }
+    }
+}
+
 /* ---------------------------------------------------------------- tile keys --- */
 
 /* The cell-tile key of each marker: the anchor node of its stencil along each axis

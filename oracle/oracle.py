@@ -4,7 +4,7 @@ Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg import 
 module, as the checker; the product (``mpifield_b200``) never does.
 
 - `gather`, `scatter`, `deposit_whitney`, `deposit_spline`, `gather_edges`,
-  `gather_grad`, `tile_keys`: the serial C restatement in ``mpf_oracle.c`` of the
+  `gather_forms`, `scatter_forms`, `gather_grad`, `tile_keys`: the serial C restatement in ``mpf_oracle.c`` of the
   reference kernels (citations there).
 - `divergence_block`, `gradient_block`: ``EdgeWeighting.divergence_block`` and
   ``gradient_block`` of src/mpifield/edges.py:217-259, restated on NumPy.
@@ -58,6 +58,8 @@ def _declare(lib: C.CDLL) -> None:
         "og_deposit_spline": [_I, _I, _P, _L, _P, _L, _P, _L, _P, _P, _P, _P, _P],
         "og_gather_edges": [_I, _I, _P, _L, _L, _P, _P, _L, _P, _P, _P, _P],
         "og_tile_keys": [_I, _I, _I, _P, _L, _P, _L, _L, _L, _P, _P, _P, _P, _P, _I, _P],
+        "og_gather_forms": [_I, _I, _I, _P, _L, _L, _P, _L, _P, _L, _P, _P, _P, _P],
+        "og_scatter_forms": [_I, _I, _I, _P, _L, _P, _L, _L, _P, _L, _P, _P, _P, _P],
         "cb_gather": [_I, _I, _I, _P, _L, _L, _P, _L, _P, _L, _P, _P, _P, _P, _I],
         "cb_scatter": [_I, _I, _I, _P, _L, _P, _L, _L, _P, _L, _P, _P, _P, _P, _I],
         "cb_deposit_whitney": [_I, _P, _L, _P, _L, _P, _L, _P, _P, _P, _P, _P, _I],
@@ -183,6 +185,35 @@ def gather_edges(degree: int, positions, edges, geometry) -> np.ndarray:
     library().og_gather_edges(lower.size, degree, _ptr(pos), ps, n, _ptr(edges), _ptr(result), n,
                               _ptr(lower), _ptr(cell), _ptr(num), _ptr(code))
     return result
+
+
+def num_form_components(form: int, ndim: int) -> int:
+    """The components of a ``form``-form in ``ndim`` dimensions (spline_forms.py:43-48)."""
+    return {(1, 1): 1, (1, 2): 2, (2, 2): 1, (1, 3): 3, (2, 3): 3, (3, 3): 1}[(form, ndim)]
+
+
+def gather_forms(degree: int, form: int, positions, field: np.ndarray, geometry) -> np.ndarray:
+    """``result (ncomp, N)`` of the reference k-form gather (gather_forms_spline)."""
+    lower, cell, num, code = split_geometry(geometry)
+    pos, ps = _rows(positions)
+    field = np.ascontiguousarray(field, dtype=np.float64)
+    ncomp = field.shape[-1]
+    n = pos.shape[1]
+    result = np.zeros((ncomp, n))
+    library().og_gather_forms(lower.size, degree, form, _ptr(pos), ps, n, _ptr(field), ncomp, _ptr(result), n,
+                              _ptr(lower), _ptr(cell), _ptr(num), _ptr(code))
+    return result
+
+
+def scatter_forms(degree: int, form: int, positions, values, field: np.ndarray, geometry) -> np.ndarray:
+    """Add the reference k-form deposit of ``values (ncomp, N)`` to ``field`` (in place); returns it."""
+    lower, cell, num, code = split_geometry(geometry)
+    pos, ps = _rows(positions)
+    vals, vs = _rows(values)
+    assert field.flags.c_contiguous and field.dtype == np.float64
+    library().og_scatter_forms(lower.size, degree, form, _ptr(pos), ps, _ptr(vals), vs, pos.shape[1], _ptr(field),
+                               field.shape[-1], _ptr(lower), _ptr(cell), _ptr(num), _ptr(code))
+    return field
 
 
 def tile_keys(kind, degree: int, positions, geometry, tile, values=None, within: bool = False) -> np.ndarray:

@@ -13,7 +13,7 @@ stub whose ``method(...)`` returns its function unchanged. Nothing else of the
 reference is stubbed: the arithmetic is that of
 ``src/mpifield/kernels/<name>/<name>_numpy.py`` and the modules they import
 (``linear_cell.py``, ``quadratic_cell.py``, ``spline_cell.py``, ``whitney_cell.py``,
-``spline_edges.py``).
+``spline_edges.py``, ``spline_forms.py``).
 
 The fixtures are small seeded cases (a few dozen markers or paths on grids of a few
 nodes per axis) covering every weighting, dimension and boundary code, with markers
@@ -187,12 +187,50 @@ def path_cases(rng) -> dict[str, np.ndarray]:
     return out
 
 
+def form_cases(rng) -> dict[str, np.ndarray]:
+    """The k-form gathers and scatters (gather_forms_spline_{n}d, scatter_forms_spline_{n}d):
+    every form of 1D to 3D, degrees 1 to 3, bounded, periodic, mixed and clamped axes."""
+    out = {}
+    for degree, ndim in itertools.product((1, 2, 3), (1, 2, 3)):
+        for form in range(1, ndim + 1):
+            code_sets = [(0,) * ndim, (1,) * ndim]
+            if ndim > 1:
+                code_sets.append((1,) + (0,) * (ndim - 1))
+            code_sets.append((2,) + (1,) * (ndim - 1))
+            for codes in code_sets:
+                tag = f"forms{degree}_{form}of{ndim}d_" + "".join(map(str, codes))
+                num = SHAPES[ndim]
+                ext = tuple(n + (degree - 1 if c == 2 else 0) for n, c in zip(num, codes))
+                ncomp = {(1, 1): 1, (1, 2): 2, (2, 2): 1, (1, 3): 3, (2, 3): 3, (3, 3): 1}[(form, ndim)]
+                geometry = (*LOWER[:ndim], *CELL[:ndim], *num, *codes)
+                count = 30
+                pos = _positions(rng, ndim, num, codes, count)
+                field = rng.normal(size=(*ext, ncomp))
+                values = rng.uniform(0.5, 1.5, (ncomp, count))
+                values[:, -3:] = 0.0
+                dead = pos.copy()
+                dead[:, -3:] = np.nan  # dead markers: zero values, any position
+                result = np.zeros((ncomp, count))
+                deposit = np.zeros((*ext, ncomp))
+                kernel(f"gather_forms_spline_{ndim}d")(pos, field, result, *geometry, degree, form)
+                kernel(f"scatter_forms_spline_{ndim}d")(dead, values, deposit, *geometry, degree, form)
+                out[f"{tag}/geometry"] = np.array(geometry, dtype=float)
+                out[f"{tag}/positions"] = pos
+                out[f"{tag}/dead_positions"] = dead
+                out[f"{tag}/field"] = field
+                out[f"{tag}/values"] = values
+                out[f"{tag}/gather"] = result
+                out[f"{tag}/scatter"] = deposit
+    return out
+
+
 def main() -> None:
     _load_reference()
     rng = np.random.default_rng(20240611)
     np.savez_compressed(OUT / "node_kernels.npz", **node_cases(rng))
     np.savez_compressed(OUT / "path_kernels.npz", **path_cases(rng))
-    for name in ("node_kernels.npz", "path_kernels.npz"):
+    np.savez_compressed(OUT / "form_kernels.npz", **form_cases(np.random.default_rng(20261204)))
+    for name in ("node_kernels.npz", "path_kernels.npz", "form_kernels.npz"):
         print(name, (OUT / name).stat().st_size, "bytes")
 
 

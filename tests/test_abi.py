@@ -190,8 +190,10 @@ def test_splines_pair_the_weightings():
     assert mf.splines(2).nodes is mf.QUADRATIC and mf.splines(2).edges is mf.QUADRATIC_EDGES
     assert mf.splines(3).nodes is mf.CUBIC and mf.splines(3).edges is mf.CUBIC_EDGES
     assert [mf.splines(p).halo for p in (1, 2, 3)] == [1, 2, 2]
-    assert repr(mf.splines(1)) == "Splines(degree 1: nodes='linear', edges='whitney')"
-    assert mf.splines(1).forms() == (mf.LINEAR, mf.WHITNEY)
+    assert repr(mf.splines(1)) == ("Splines(degree 1: nodes='linear', edges='whitney', faces='linear faces', "
+                                   "cells='linear cells')")
+    assert mf.splines(1).forms()[:2] == (mf.LINEAR, mf.WHITNEY)
+    assert mf.splines(2).faces.dimensions() == (3,) and mf.splines(2).cells.dimensions() == (1, 2, 3)
     assert all(w.clamps for w in mf.splines(1, clamped=True).forms())
     with pytest.raises(ValueError, match="no built-in splines of degree 5"):
         mf.splines(5)
@@ -222,5 +224,5 @@ def test_the_catalog_has_the_reference_kernel_names():
     for n in (1, 2, 3):
         for name in ("gather_linear", "scatter_linear", "gather_quadratic", "scatter_quadratic", "gather_spline",
                      "scatter_spline", "deposit_paths", "deposit_paths_spline", "gather_edges",
-                     "gather_edges_spline"):
+                     "gather_edges_spline", "gather_forms_spline", "scatter_forms_spline"):
             assert f"{name}_{n}d" in mf.KERNELS

@@ -132,7 +132,9 @@ def reference():
     _load("mpifield._types", SRC / "mpifield" / "_types.py")
     weighting = _load("mpifield.weighting", SRC / "mpifield" / "weighting.py")
     edges = _load("mpifield.edges", SRC / "mpifield" / "edges.py")
-    yield types.SimpleNamespace(weighting=weighting, edges=edges, types=sys.modules["mpifield._types"])
+    splines = _load("mpifield.splines", SRC / "mpifield" / "splines.py")
+    yield types.SimpleNamespace(weighting=weighting, edges=edges, splines=splines,
+                                types=sys.modules["mpifield._types"])
     sys.modules.clear()
     sys.modules.update(saved)
 
@@ -172,6 +174,20 @@ class OracleLibrary:
             self.oracle.og_deposit_whitney(ndim, s, ss, e, es, q, n, edges, *geometry)
         else:
             self.oracle.og_deposit_spline(ndim, degree, s, ss, e, es, q, n, edges, *geometry)
+        return 0
+
+    def mpf_gather_forms(self, degree, form, ndim, pos, ps, n, field, ncomp, out, rs, lower, cell, num, code, dtype,
+                         stream):
+        self._record("gather_forms", (degree, form, ndim, ps, n, ncomp, rs, dtype, stream))
+        self.oracle.og_gather_forms(ndim, degree, form, pos, ps, n, field, ncomp, out, rs, C.addressof(lower),
+                                    C.addressof(cell), C.addressof(num), C.addressof(code))
+        return 0
+
+    def mpf_scatter_forms(self, degree, form, ndim, pos, ps, vals, vs, n, field, ncomp, lower, cell, num, code,
+                          dtype, stream):
+        self._record("scatter_forms", (degree, form, ndim, ps, vs, n, ncomp, dtype, stream))
+        self.oracle.og_scatter_forms(ndim, degree, form, pos, ps, vals, vs, n, field, ncomp, C.addressof(lower),
+                                     C.addressof(cell), C.addressof(num), C.addressof(code))
         return 0
 
     def mpf_gather_edges(self, kind, degree, ndim, pos, ps, n, edges, out, rs, lower, cell, num, code, dtype,
@@ -287,3 +303,25 @@ def test_our_block_types_accept_interface_arrays(recorder):
     mf.QUADRATIC.scatter_block(FakeDeviceArray(pos), FakeDeviceArray(np.ones(100)), FakeDeviceArray(field), grid)
     expected = O.scatter("quadratic", 2, pos, np.ones((1, 100)), np.zeros_like(field), grid.geometry)
     assert rel_err(field, expected) <= RTOL_F64
+
+
+@pytest.mark.parametrize("degree", [1, 2, 3])
+def test_the_reference_faces_and_cells_on_our_kernels(reference, recorder, degree):
+    # mpifield's own Splines (src/mpifield/splines.py:185-205) built from our form kernels
+    rng = np.random.default_rng(60 + degree)
+    sp = reference.splines.SPLINES[degree]
+    grid = _grid(reference, 3, True)
+    pos, values = _markers(rng, grid, 300, 3)
+    faces = np.zeros((9, 7, 6, 3))
+    sp.faces.scatter_block(FakeDeviceArray(pos), FakeDeviceArray(values), FakeDeviceArray(faces), grid)
+    expected = O.scatter_forms(degree, 2, pos, np.ascontiguousarray(values), np.zeros_like(faces), grid.geometry)
+    assert rel_err(faces, expected) <= RTOL_F64
+    for ndim in (1, 2, 3):
+        g = _grid(reference, ndim, False)
+        p, _ = _markers(rng, g, 200, 1)
+        shape = tuple(int(n) for n in g.num_gridpoints)
+        cells = rng.normal(size=shape + (1,))
+        result = np.zeros((1, 200))
+        sp.cells.gather_block(FakeDeviceArray(p), FakeDeviceArray(cells), FakeDeviceArray(result), g)
+        assert rel_err(result, O.gather_forms(degree, ndim, p, cells, g.geometry)) <= RTOL_F64
+    assert {c[0] for c in recorder.calls} == {"scatter_forms", "gather_forms"}

@@ -23,6 +23,7 @@ from tests.helpers import cases, geometry, load, node_case, rel_err
 
 NODES = load("node_kernels.npz")
 PATHS = load("path_kernels.npz")
+FORMS = load("form_kernels.npz")
 
 
 @pytest.mark.parametrize("tag", cases(NODES))
@@ -51,6 +52,23 @@ def test_path_oracle_matches_the_reference_numpy_kernels(tag):
         np.testing.assert_allclose(whitney, PATHS[f"{tag}/whitney"], rtol=0, atol=1e-13)
         field = O.gather_edges(0, PATHS[f"{tag}/points"], PATHS[f"{tag}/edges"], geom)
         np.testing.assert_allclose(field, PATHS[f"{tag}/whitney_gather"], rtol=0, atol=1e-12)
+
+
+def _form_case(tag):
+    """(degree, form, ndim) of a k-form fixture tag such as ``forms2_1of3d_111``."""
+    head = tag.split("_")
+    return int(head[0][5:]), int(head[1][0]), int(head[1][3])
+
+
+@pytest.mark.parametrize("tag", cases(FORMS))
+def test_form_oracle_matches_the_reference_numpy_kernels(tag):
+    degree, form, _ = _form_case(tag)
+    geom = geometry(FORMS[f"{tag}/geometry"])
+    result = O.gather_forms(degree, form, FORMS[f"{tag}/positions"], FORMS[f"{tag}/field"], geom)
+    np.testing.assert_allclose(result, FORMS[f"{tag}/gather"], rtol=0, atol=1e-13)
+    deposit = np.zeros_like(FORMS[f"{tag}/field"])
+    O.scatter_forms(degree, form, FORMS[f"{tag}/dead_positions"], FORMS[f"{tag}/values"], deposit, geom)
+    np.testing.assert_allclose(deposit, FORMS[f"{tag}/scatter"], rtol=0, atol=1e-13)
 
 
 # ------------------------------------------------ the reference compiled as C++ --
@@ -119,6 +137,33 @@ def test_path_oracle_is_the_reference_cuda_arithmetic(ndim, degree):
             mine = np.zeros_like(expected)
             O.deposit_whitney(start, end, charges, mine, geom)
             np.testing.assert_allclose(mine, expected, rtol=0, atol=1e-14)
+
+
+@needs_ref
+@pytest.mark.parametrize("ndim", [1, 2, 3])
+@pytest.mark.parametrize("degree", [1, 2, 3])
+def test_form_oracle_is_the_reference_cuda_arithmetic(ndim, degree):
+    rng = np.random.default_rng(200 + degree + 10 * ndim)
+    ref = O.RefHost()
+    for form in range(1, ndim + 1):
+        ncomp = O.num_form_components(form, ndim)
+        for codes in ((0,) * ndim, (1,) * ndim, (2,) + (1,) * (ndim - 1)):
+            shape = (9, 8, 7)[:ndim]
+            ext = tuple(s + (degree - 1 if c == 2 else 0) for s, c in zip(shape, codes))
+            geom = (*rng.uniform(-1, 1, ndim), *rng.uniform(0.2, 0.5, ndim), *shape, *codes)
+            lower = np.array(geom[:ndim])
+            cell = np.array(geom[ndim:2 * ndim])
+            pos = lower[:, None] + cell[:, None] * rng.uniform(-2, np.array(shape)[:, None] + 1, (ndim, 200))
+            field = rng.normal(size=(*ext, ncomp))
+            expected = np.zeros((ncomp, 200))
+            ref.call(f"gather_forms_spline_{ndim}d", 200, pos, field, expected, *geom, degree, form)
+            np.testing.assert_allclose(O.gather_forms(degree, form, pos, field, geom), expected, rtol=0, atol=1e-14)
+            values = rng.uniform(0.5, 1.5, (ncomp, 200))
+            deposit = np.zeros_like(field)
+            ref.call(f"scatter_forms_spline_{ndim}d", 200, pos, values, deposit, *geom, degree, form)
+            mine = np.zeros_like(field)
+            O.scatter_forms(degree, form, pos, values, mine, geom)
+            np.testing.assert_allclose(mine, deposit, rtol=0, atol=1e-14)
 
 
 # --------------------------------------------------------------- known answers --
