@@ -20,11 +20,14 @@ static int run_deposit(PathArgs<T> a, const Tuning& t, cudaStream_t stream) {
         };
         // two CTAs per SM (128 registers a thread) where the path fits them without spills
         // (WHITNEY and spline edges of degree <= 2: QUADRATIC_EDGES 15% faster than one);
-        // the cubic edges keep one CTA and their registers. Variant 1: one CTA everywhere.
+        // the cubic edges keep one CTA and their registers. Variant 1: one CTA everywhere;
+        // variant 3: spline paths a path at a time instead of piece by piece.
         if constexpr (!WHITNEY && P >= 3) {
-            launch(deposit_paths_kernel<T, NDIM, P, WHITNEY, 256, 1>, 256);
+            if (t.variant == 3) launch(deposit_paths_kernel<T, NDIM, P, WHITNEY, 256, 1, false>, 256);
+            else launch(deposit_paths_kernel<T, NDIM, P, WHITNEY, 256, 1>, 256);
         } else {
             if (t.variant == 1) launch(deposit_paths_kernel<T, NDIM, P, WHITNEY, 256, 1>, 256);
+            else if (t.variant == 3) launch(deposit_paths_kernel<T, NDIM, P, WHITNEY, 256, 2, false>, 256);
             else launch(deposit_paths_kernel<T, NDIM, P, WHITNEY, 256, 2>, 256);
         }
         count_launches(1);

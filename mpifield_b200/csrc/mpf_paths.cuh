@@ -34,6 +34,11 @@ namespace mpf {
 // cells per step) never reach it.
 constexpr int kMaxPathSteps = 1 << 16;
 
+// RN(1 / x), the correctly rounded reciprocal (the divisor table of div_rn).
+template <typename T> __device__ __forceinline__ T recip_rn(T x);
+template <> __device__ __forceinline__ double recip_rn<double>(double x) { return __drcp_rn(x); }
+template <> __device__ __forceinline__ float recip_rn<float>(float x) { return __frcp_rn(x); }
+
 template <typename T> __device__ __forceinline__ T clamp_to_axis(T rel, int num, int code) {
     if (code == PERIODIC) return rel;
     if (rel < T(0)) return T(0);
@@ -65,10 +70,13 @@ __device__ __forceinline__ void linear_nodes(T rel, int num, int code, int& left
 
 template <typename T, int NDIM, typename Sink>
 __device__ void whitney_path(T q, const T* a, const T* b, const Grid<T>& g, const Sink& sink) {
-    T dl[NDIM], plane[NDIM], step[NDIM], p0[NDIM];
+    // the crossing times (plane - a) / dl are correctly rounded quotients from RN(1 / dl)
+    // (div_rn): the bits of the division, without a division per cut
+    T dl[NDIM], rdl[NDIM], plane[NDIM], step[NDIM], p0[NDIM];
 #pragma unroll
     for (int d = 0; d < NDIM; ++d) {
         dl[d] = b[d] - a[d];
+        rdl[d] = recip_rn(dl[d]);
         if (dl[d] < T(0)) {
             plane[d] = ceil(a[d]) - T(1);
             step[d] = T(-1);
@@ -84,7 +92,7 @@ __device__ void whitney_path(T q, const T* a, const T* b, const Grid<T>& g, cons
         T following = T(1);
 #pragma unroll
         for (int d = 0; d < NDIM; ++d) {
-            times[d] = dl[d] != T(0) ? (plane[d] - a[d]) / dl[d] : T(2);
+            times[d] = dl[d] != T(0) ? div_rn(plane[d] - a[d], dl[d], rdl[d]) : T(2);
             if (times[d] < following) following = times[d];
         }
         T p1[NDIM], f[NDIM], delta[NDIM];
@@ -112,7 +120,7 @@ __device__ void whitney_path(T q, const T* a, const T* b, const Grid<T>& g, cons
                 // the two axes across this one, in increasing order
                 const int ua = axis == 0 ? 1 : 0;
                 const int wa = axis == 2 ? 1 : 2;
-                const T cross = delta[ua] * delta[wa] / T(12);
+                const T cross = div_rn(delta[ua] * delta[wa], T(12), T(1) / T(12));
                 const T along = q * delta[axis];
 #pragma unroll
                 for (int u = 0; u < 2; ++u)
@@ -237,13 +245,18 @@ template <typename T> struct Gauss<T, 5> {
 };
 
 // The ascending crossing times of one axis over a stretch: knot planes first..last
-// walked in the direction of increasing time, then merged with the two wall times.
+// walked in the direction of increasing time, then merged with the two wall times. The
+// times are correctly rounded quotients (div_rn with RN(1 / delta)), the bits of the
+// division; the pending walls are a queue of 2-bit codes (1: the wall at 0, 2: the wall
+// at num - 1), their times computed when looked at.
 template <typename T> struct CutStream {
     T a0, delta, plane;
     int left;   // planes not yet taken
-    T stepdir;  // +1 or -1
-    T wall[2];
-    int walls;  // walls not yet taken (taken from wall[2 - walls])
+    int walls;  // the pending walls, the next in the low two bits
+
+    __device__ __forceinline__ T wall_time(int code, int num) const {
+        return div_rn((code == 1 ? T(0) : T(num) - T(1)) - a0, delta, recip_rn(delta));
+    }
 
     __device__ __forceinline__ void init(T s0, T s1, T shift, int num, int code) {
         a0 = s0;
@@ -251,7 +264,6 @@ template <typename T> struct CutStream {
         left = 0;
         walls = 0;
         plane = T(0);
-        stepdir = T(1);
         if (delta == T(0)) return;
         const T low = delta > T(0) ? s0 : s1;
         const T high = delta > T(0) ? s1 : s0;
@@ -260,239 +272,298 @@ template <typename T> struct CutStream {
         int count = 0;
         while (first + T(count) < high && count < 64) ++count;
         left = count;
-        if (delta > T(0)) {
-            plane = first;
-            stepdir = T(1);
-        } else {
-            plane = first + T(count - 1);
-            stepdir = T(-1);
-        }
+        plane = delta > T(0) ? first : first + T(count - 1);
         if (code != PERIODIC) {
-            T t0 = (T(0) - s0) / delta;
-            T t1 = (T(num) - T(1) - s0) / delta;
+            const T t0 = wall_time(1, num);
+            const T t1 = wall_time(2, num);
             const bool in0 = t0 > T(0) && t0 < T(1);
             const bool in1 = t1 > T(0) && t1 < T(1);
-            if (in0 && in1) {
-                wall[0] = t0 < t1 ? t0 : t1;
-                wall[1] = t0 < t1 ? t1 : t0;
-                walls = 2;
-            } else if (in0 || in1) {
-                wall[1] = in0 ? t0 : t1;
-                walls = 1;
-            }
+            if (in0 && in1) walls = t0 < t1 ? (1 | 2 << 2) : (2 | 1 << 2);
+            else if (in0) walls = 1;
+            else if (in1) walls = 2;
         }
+    }
+    // The next plane in the direction of increasing time (delta > 0: up).
+    __device__ __forceinline__ void advance() {
+        plane += delta > T(0) ? T(1) : T(-1);
+        --left;
     }
     // The next plane time inside (0, 1), skipping the ones rounding outside.
     __device__ __forceinline__ T peek_plane() {
-        while (left > 0) {
-            const T t = (plane - a0) / delta;
-            if (t > T(0) && t < T(1)) return t;
-            plane += stepdir;
-            --left;
+        if (left > 0) {
+            const T rd = recip_rn(delta);
+            while (left > 0) {
+                const T t = div_rn(plane - a0, delta, rd);
+                if (t > T(0) && t < T(1)) return t;
+                advance();
+            }
         }
         return T(2);
     }
-    __device__ __forceinline__ T peek_wall() const { return walls > 0 ? wall[2 - walls] : T(2); }
+    __device__ __forceinline__ T peek_wall(int num) const { return walls ? wall_time(walls & 3, num) : T(2); }
+    __device__ __forceinline__ void pop_wall() { walls >>= 2; }
 };
 
+// One piece of a spline path: q times the line integral of the edge functions from p0
+// to p0 + step (cell coordinates, clamped on bounded axes), added to the sink.
 template <typename T, int NDIM, int P, typename Sink>
-__device__ void spline_path(T q, const T* r0, const T* r1, const Grid<T>& g, const Sink& sink) {
+__device__ __forceinline__ void spline_piece(T q, const T* p0, const T* step, const Grid<T>& g, bool clamped,
+                                             const Sink& sink) {
     constexpr int NPTS = (P - 1 + (NDIM - 1) * P) / 2 + 1;
-    const T shift = (P % 2 == 0) ? T(0.5) : T(0);
-    T extent = T(0);
+    if (!clamped) {
+        // The Gauss points of a piece lie in one knot interval on every axis:
+        // the nodes, the edges and their existence are those of the piece's
+        // midpoint, and a point's weights are the stencil polynomials at the
+        // midpoint's offset plus (point - 1/2) times the step. The contributions
+        // of the points are summed in registers, one atomic per edge and axis.
+        int sidx[3][P + 1], aidx[3][P > 0 ? P : 1];
+        bool aex[3][P > 0 ? P : 1];
+        T st[3], at[3];
 #pragma unroll
-    for (int d = 0; d < NDIM; ++d) {
-        const T span = r1[d] > r0[d] ? r1[d] - r0[d] : r0[d] - r1[d];
-        if (span > extent) extent = span;
+        for (int d = 0; d < NDIM; ++d) {
+            const T mid = p0[d] + T(0.5) * step[d];
+            const int first = spline_frame<T, P>(mid, g.num[d], g.code[d], st[d]);
+#pragma unroll
+            for (int s = 0; s <= P; ++s) sidx[d][s] = map_node(first + s, g.num[d], g.code[d]);
+            along_frame<T, P>(mid, g.num[d], g.code[d], aidx[d], aex[d], at[d]);
+        }
+        constexpr int SX = P + 1;
+        constexpr int CB = NDIM > 1 ? SX : 1;
+        constexpr int CC = NDIM > 2 ? SX : 1;
+#pragma unroll
+        for (int axis = 0; axis < NDIM; ++axis) {
+            if (q * step[axis] == T(0)) continue;
+            // the axes across this one, in increasing order
+            const int o1 = NDIM > 1 ? (axis == 0 ? 1 : 0) : 0;
+            const int o2 = NDIM > 2 ? (axis == 2 ? 1 : 2) : 0;
+            // one edge along the axis at a time: (P + 1)^(ndim - 1) sums
+#pragma unroll
+            for (int e = 0; e < P; ++e) {
+                if (!aex[axis][e]) continue;
+                T acc[CB * CC];
+#pragma unroll
+                for (int k = 0; k < CB * CC; ++k) acc[k] = T(0);
+#pragma unroll
+                for (int gp = 0; gp < NPTS; ++gp) {
+                    const T off = Gauss<T, NPTS>::point(gp) - T(0.5);
+                    T wa[P > 0 ? P : 1], wb[SX], wc[SX];
+                    uniform_weights<T, P - 1>(at[axis] + off * step[axis], wa);
+                    if constexpr (NDIM > 1) uniform_weights<T, P>(st[o1] + off * step[o1], wb);
+                    if constexpr (NDIM > 2) uniform_weights<T, P>(st[o2] + off * step[o2], wc);
+                    const T along = q * Gauss<T, NPTS>::weight(gp) * step[axis] * wa[e];
+#pragma unroll
+                    for (int b = 0; b < CB; ++b) {
+                        const T wab = NDIM > 1 ? along * wb[b] : along;
+#pragma unroll
+                        for (int c = 0; c < CC; ++c) {
+                            T& r = acc[b * CC + c];
+                            if constexpr (NDIM > 2) r = fma(wab, wc[c], r);
+                            else r = r + wab;
+                        }
+                    }
+                }
+#pragma unroll
+                for (int b = 0; b < CB; ++b)
+#pragma unroll
+                    for (int c = 0; c < CC; ++c) {
+                        int n[3] = {0, 0, 0};
+                        n[axis] = aidx[axis][e];
+                        if constexpr (NDIM > 1) n[o1] = sidx[o1][b];
+                        if constexpr (NDIM > 2) n[o2] = sidx[o2][c];
+                        sink.add(n, axis, acc[b * CC + c]);
+                    }
+            }
+        }
+    } else {
+        // clamped knots: every Gauss point computes its full stencil (Cox-de Boor
+        // near the walls) and adds its own contributions
+#pragma unroll
+        for (int gp = 0; gp < NPTS; ++gp) {
+            const T point = Gauss<T, NPTS>::point(gp);
+            const T gw = Gauss<T, NPTS>::weight(gp);
+            T rel[NDIM];
+#pragma unroll
+            for (int d = 0; d < NDIM; ++d) rel[d] = p0[d] + point * step[d];
+#pragma unroll 1
+            for (int axis = 0; axis < NDIM; ++axis) {
+                const T amount = q * gw * step[axis];
+                if (amount == T(0)) continue;
+                int idx[3][P + 1];
+                T wt[3][P + 1];
+                bool ex[P > 0 ? P : 1];
+#pragma unroll
+                for (int d = 0; d < NDIM; ++d) {
+                    if (d == axis) {
+                        along_stencil<T, P>(rel[d], g.num[d], g.code[d], idx[d], wt[d], ex);
+                    } else {
+                        const int base = axis_stencil<T, SPLINE, P>(rel[d], g.num[d], g.code[d], wt[d]);
+#pragma unroll
+                        for (int s2 = 0; s2 <= P; ++s2) idx[d][s2] = map_node(base + s2, g.num[d], g.code[d]);
+                    }
+                }
+                const int cnt0 = axis == 0 ? P : P + 1;
+                const int cnt1 = NDIM > 1 ? (axis == 1 ? P : P + 1) : 1;
+                const int cnt2 = NDIM > 2 ? (axis == 2 ? P : P + 1) : 1;
+                for (int x = 0; x < cnt0; ++x) {
+                    if (axis == 0 && !ex[x]) continue;
+                    for (int y = 0; y < cnt1; ++y) {
+                        if (NDIM > 1 && axis == 1 && !ex[y]) continue;
+                        for (int z = 0; z < cnt2; ++z) {
+                            if (NDIM > 2 && axis == 2 && !ex[z]) continue;
+                            T w = amount * wt[0][x];
+                            if constexpr (NDIM > 1) w = w * wt[1][y];
+                            if constexpr (NDIM > 2) w = w * wt[2][z];
+                            int n[3] = {idx[0][x], NDIM > 1 ? idx[1][y] : 0, NDIM > 2 ? idx[2][z] : 0};
+                            sink.add(n, axis, w);
+                        }
+                    }
+                }
+            }
+        }
     }
+}
+
+// The pieces of a spline path, one at a time: stretches of at most 4 cells, each cut at
+// its knot planes and walls in ascending time (the merged CutStreams). begin() starts a
+// path at its first stretch; piece() takes the next cut and returns true with the piece
+// (p0, step) when it has a length, and sets `ended` after the stretch's last cut; then
+// more() tells whether another stretch follows, which next() starts (the path's ends
+// given again: the walk does not keep them). live turns false after the last stretch.
+template <typename T, int NDIM, int P> struct SplineWalk {
+    CutStream<T> cs[NDIM];  // cs[d].a0, cs[d].delta: the stretch's start and extent per axis
+    T t0;
+    int st, stretches, guard;
+    bool live, ended;
+
+    __device__ __forceinline__ void start_stretch(const T* r0, const T* r1, const Grid<T>& g) {
+        const T shift = (P % 2 == 0) ? T(0.5) : T(0);
+#pragma unroll
+        for (int d = 0; d < NDIM; ++d) {
+            // (x / 1 is x: one stretch, the usual case, divides nothing)
+            const T u0 = (r1[d] - r0[d]) * T(st), u1 = (r1[d] - r0[d]) * T(st + 1);
+            cs[d].init(r0[d] + (stretches == 1 ? u0 : u0 / T(stretches)),
+                       r0[d] + (stretches == 1 ? u1 : u1 / T(stretches)), shift, g.num[d], g.code[d]);
+        }
+        t0 = T(0);
+        guard = 0;
+        ended = false;
+    }
+
+    __device__ __forceinline__ void begin(const T* r0, const T* r1, const Grid<T>& g) {
+        T extent = T(0);
+#pragma unroll
+        for (int d = 0; d < NDIM; ++d) {
+            const T span = r1[d] > r0[d] ? r1[d] - r0[d] : r0[d] - r1[d];
+            if (span > extent) extent = span;
+        }
+        stretches = trunc_int<T>(extent / T(4)) + 1;
+        if (stretches > kMaxPathSteps || stretches < 1) stretches = kMaxPathSteps;
+        st = 0;
+        live = true;
+        start_stretch(r0, r1, g);
+    }
+
+    __device__ __forceinline__ bool more() const { return st + 1 < stretches; }
+
+    __device__ __forceinline__ void next(const T* r0, const T* r1, const Grid<T>& g) {
+        ++st;
+        start_stretch(r0, r1, g);
+    }
+
+    __device__ __forceinline__ bool piece(const Grid<T>& g, T* p0, T* step) {
+        // the next cut: the least pending time of every stream, or the end
+        T t1 = T(1);
+        int which = -1;
+#pragma unroll
+        for (int d = 0; d < NDIM; ++d) {
+            const T tp = cs[d].peek_plane();
+            if (tp < t1) { t1 = tp; which = 2 * d; }
+            const T tw = cs[d].peek_wall(g.num[d]);
+            if (tw < t1) { t1 = tw; which = 2 * d + 1; }
+        }
+        if (which >= 0) {
+#pragma unroll
+            for (int d = 0; d < NDIM; ++d) {
+                if (which == 2 * d) cs[d].advance();
+                if (which == 2 * d + 1) cs[d].pop_wall();
+            }
+        }
+        const bool length = t1 > t0;
+        if (length) {
+#pragma unroll
+            for (int d = 0; d < NDIM; ++d) {
+                T begin_ = cs[d].a0 + t0 * cs[d].delta;
+                T finish = cs[d].a0 + t1 * cs[d].delta;
+                if (g.code[d] != PERIODIC) {
+                    const T top = T(g.num[d] - 1);
+                    if (begin_ < T(0)) begin_ = T(0);
+                    if (begin_ > top) begin_ = top;
+                    if (finish < T(0)) finish = T(0);
+                    if (finish > top) finish = top;
+                }
+                p0[d] = begin_;
+                step[d] = finish - begin_;
+            }
+        }
+        t0 = t1;
+        if (which < 0 || ++guard >= 64) ended = true;  // the stretch is done
+        return length;
+    }
+};
+
+// Whether any axis has clamped knots.
+template <typename T, int NDIM> __device__ __forceinline__ bool any_clamped(const Grid<T>& g) {
     bool clamped = false;
 #pragma unroll
     for (int d = 0; d < NDIM; ++d) clamped = clamped || g.code[d] == CLAMPED;
-    int stretches = trunc_int<T>(extent / T(4)) + 1;
-    if (stretches > kMaxPathSteps || stretches < 1) stretches = kMaxPathSteps;
-    for (int st = 0; st < stretches; ++st) {
-        T a0[NDIM], a1[NDIM];
-        CutStream<T> cs[NDIM];
-#pragma unroll
-        for (int d = 0; d < NDIM; ++d) {
-            a0[d] = r0[d] + (r1[d] - r0[d]) * T(st) / T(stretches);
-            a1[d] = r0[d] + (r1[d] - r0[d]) * T(st + 1) / T(stretches);
-            cs[d].init(a0[d], a1[d], shift, g.num[d], g.code[d]);
-        }
-        T t0 = T(0);
-        for (int guard = 0; guard < 64; ++guard) {
-            // the next cut: the least pending time of every stream, or the end
-            T t1 = T(1);
-            int which = -1;
-#pragma unroll
-            for (int d = 0; d < NDIM; ++d) {
-                const T tp = cs[d].peek_plane();
-                if (tp < t1) { t1 = tp; which = 2 * d; }
-                const T tw = cs[d].peek_wall();
-                if (tw < t1) { t1 = tw; which = 2 * d + 1; }
-            }
-            if (which >= 0) {
-#pragma unroll
-                for (int d = 0; d < NDIM; ++d) {
-                    if (which == 2 * d) { cs[d].plane += cs[d].stepdir; --cs[d].left; }
-                    if (which == 2 * d + 1) --cs[d].walls;
-                }
-            }
-            if (t1 > t0) {
-                T p0[NDIM], step[NDIM];
-#pragma unroll
-                for (int d = 0; d < NDIM; ++d) {
-                    T begin = a0[d] + t0 * (a1[d] - a0[d]);
-                    T finish = a0[d] + t1 * (a1[d] - a0[d]);
-                    if (g.code[d] != PERIODIC) {
-                        const T top = T(g.num[d] - 1);
-                        if (begin < T(0)) begin = T(0);
-                        if (begin > top) begin = top;
-                        if (finish < T(0)) finish = T(0);
-                        if (finish > top) finish = top;
-                    }
-                    p0[d] = begin;
-                    step[d] = finish - begin;
-                }
-                if (!clamped) {
-                    // The Gauss points of a piece lie in one knot interval on every axis:
-                    // the nodes, the edges and their existence are those of the piece's
-                    // midpoint, and a point's weights are the stencil polynomials at the
-                    // midpoint's offset plus (point - 1/2) times the step. The contributions
-                    // of the points are summed in registers, one atomic per edge and axis.
-                    int sidx[3][P + 1], aidx[3][P > 0 ? P : 1];
-                    bool aex[3][P > 0 ? P : 1];
-                    T st[3], at[3];
-#pragma unroll
-                    for (int d = 0; d < NDIM; ++d) {
-                        const T mid = p0[d] + T(0.5) * step[d];
-                        const int first = spline_frame<T, P>(mid, g.num[d], g.code[d], st[d]);
-#pragma unroll
-                        for (int s = 0; s <= P; ++s) sidx[d][s] = map_node(first + s, g.num[d], g.code[d]);
-                        along_frame<T, P>(mid, g.num[d], g.code[d], aidx[d], aex[d], at[d]);
-                    }
-                    constexpr int SX = P + 1;
-                    constexpr int CB = NDIM > 1 ? SX : 1;
-                    constexpr int CC = NDIM > 2 ? SX : 1;
-#pragma unroll
-                    for (int axis = 0; axis < NDIM; ++axis) {
-                        if (q * step[axis] == T(0)) continue;
-                        // the axes across this one, in increasing order
-                        const int o1 = NDIM > 1 ? (axis == 0 ? 1 : 0) : 0;
-                        const int o2 = NDIM > 2 ? (axis == 2 ? 1 : 2) : 0;
-                        // one edge along the axis at a time: (P + 1)^(ndim - 1) sums
-#pragma unroll
-                        for (int e = 0; e < P; ++e) {
-                            if (!aex[axis][e]) continue;
-                            T acc[CB * CC];
-#pragma unroll
-                            for (int k = 0; k < CB * CC; ++k) acc[k] = T(0);
-#pragma unroll
-                            for (int gp = 0; gp < NPTS; ++gp) {
-                                const T off = Gauss<T, NPTS>::point(gp) - T(0.5);
-                                T wa[P > 0 ? P : 1], wb[SX], wc[SX];
-                                uniform_weights<T, P - 1>(at[axis] + off * step[axis], wa);
-                                if constexpr (NDIM > 1) uniform_weights<T, P>(st[o1] + off * step[o1], wb);
-                                if constexpr (NDIM > 2) uniform_weights<T, P>(st[o2] + off * step[o2], wc);
-                                const T along = q * Gauss<T, NPTS>::weight(gp) * step[axis] * wa[e];
-#pragma unroll
-                                for (int b = 0; b < CB; ++b) {
-                                    const T wab = NDIM > 1 ? along * wb[b] : along;
-#pragma unroll
-                                    for (int c = 0; c < CC; ++c) {
-                                        T& r = acc[b * CC + c];
-                                        if constexpr (NDIM > 2) r = fma(wab, wc[c], r);
-                                        else r = r + wab;
-                                    }
-                                }
-                            }
-#pragma unroll
-                            for (int b = 0; b < CB; ++b)
-#pragma unroll
-                                for (int c = 0; c < CC; ++c) {
-                                    int n[3] = {0, 0, 0};
-                                    n[axis] = aidx[axis][e];
-                                    if constexpr (NDIM > 1) n[o1] = sidx[o1][b];
-                                    if constexpr (NDIM > 2) n[o2] = sidx[o2][c];
-                                    sink.add(n, axis, acc[b * CC + c]);
-                                }
-                        }
-                    }
-                } else {
-                    // clamped knots: every Gauss point computes its full stencil (Cox-de Boor
-                    // near the walls) and adds its own contributions
-#pragma unroll
-                    for (int gp = 0; gp < NPTS; ++gp) {
-                        const T point = Gauss<T, NPTS>::point(gp);
-                        const T gw = Gauss<T, NPTS>::weight(gp);
-                        T rel[NDIM];
-#pragma unroll
-                        for (int d = 0; d < NDIM; ++d) rel[d] = p0[d] + point * step[d];
-#pragma unroll 1
-                        for (int axis = 0; axis < NDIM; ++axis) {
-                            const T amount = q * gw * step[axis];
-                            if (amount == T(0)) continue;
-                            int idx[3][P + 1];
-                            T wt[3][P + 1];
-                            bool ex[P > 0 ? P : 1];
-#pragma unroll
-                            for (int d = 0; d < NDIM; ++d) {
-                                if (d == axis) {
-                                    along_stencil<T, P>(rel[d], g.num[d], g.code[d], idx[d], wt[d], ex);
-                                } else {
-                                    const int base = axis_stencil<T, SPLINE, P>(rel[d], g.num[d], g.code[d], wt[d]);
-#pragma unroll
-                                    for (int s2 = 0; s2 <= P; ++s2) idx[d][s2] = map_node(base + s2, g.num[d], g.code[d]);
-                                }
-                            }
-                            const int cnt0 = axis == 0 ? P : P + 1;
-                            const int cnt1 = NDIM > 1 ? (axis == 1 ? P : P + 1) : 1;
-                            const int cnt2 = NDIM > 2 ? (axis == 2 ? P : P + 1) : 1;
-                            for (int x = 0; x < cnt0; ++x) {
-                                if (axis == 0 && !ex[x]) continue;
-                                for (int y = 0; y < cnt1; ++y) {
-                                    if (NDIM > 1 && axis == 1 && !ex[y]) continue;
-                                    for (int z = 0; z < cnt2; ++z) {
-                                        if (NDIM > 2 && axis == 2 && !ex[z]) continue;
-                                        T w = amount * wt[0][x];
-                                        if constexpr (NDIM > 1) w = w * wt[1][y];
-                                        if constexpr (NDIM > 2) w = w * wt[2][z];
-                                        int n[3] = {idx[0][x], NDIM > 1 ? idx[1][y] : 0, NDIM > 2 ? idx[2][z] : 0};
-                                        sink.add(n, axis, w);
-                                    }
-                                }
-                            }
-                        }
-                    }
-                }
-                t0 = t1;
-            }
-            if (which < 0) break;
-        }
+    return clamped;
+}
+
+template <typename T, int NDIM, int P, typename Sink>
+__device__ void spline_path(T q, const T* r0, const T* r1, const Grid<T>& g, const Sink& sink) {
+    const bool clamped = any_clamped<T, NDIM>(g);
+    SplineWalk<T, NDIM, P> walk;
+    walk.begin(r0, r1, g);
+    for (;;) {
+        T p0[NDIM], step[NDIM];
+        if (walk.piece(g, p0, step)) spline_piece<T, NDIM, P>(q, p0, step, g, clamped, sink);
+        if (!walk.ended) continue;
+        if (!walk.more()) break;
+        walk.next(r0, r1, g);
     }
 }
 
 
 
-// The cell coordinates of path i's ends; false for a path whose ends are not finite
-// (it deposits nothing: src/mpifield/edges.py:87).
+// The cell coordinates r0, r1 of a path's ends s, e; false for a path whose ends are not
+// finite (it deposits nothing: src/mpifield/edges.py:87).
 template <typename T, int NDIM, bool WHITNEY>
-__device__ __forceinline__ bool path_cells(const PathArgs<T>& a, int64_t i, T* r0, T* r1) {
+__device__ __forceinline__ bool path_cells_of(const Grid<T>& g, const T* s, const T* e, T* r0, T* r1) {
     bool finite = true;
 #pragma unroll
     for (int d = 0; d < NDIM; ++d) {
-        const T s = a.start[d * a.start_stride + i];
-        const T e = a.end[d * a.end_stride + i];
-        r0[d] = cells_from(s - a.g.lower[d], a.g.cell[d], a.g.inv[d], a.g.pow2[d]);
-        r1[d] = cells_from(e - a.g.lower[d], a.g.cell[d], a.g.inv[d], a.g.pow2[d]);
+        r0[d] = cells_from(s[d] - g.lower[d], g.cell[d], g.inv[d], g.pow2[d]);
+        r1[d] = cells_from(e[d] - g.lower[d], g.cell[d], g.inv[d], g.pow2[d]);
         if constexpr (WHITNEY) {
             const T big = sizeof(T) == 8 ? T(1e300) : T(3e38);
             if (!(r0[d] > -big && r0[d] < big && r1[d] > -big && r1[d] < big)) finite = false;
         } else {
-            if (!(s - s == T(0)) || !(e - e == T(0))) finite = false;
+            if (!(s[d] - s[d] == T(0)) || !(e[d] - e[d] == T(0))) finite = false;
         }
     }
     return finite;
+}
+
+// The same for path i of the arguments.
+template <typename T, int NDIM, bool WHITNEY>
+__device__ __forceinline__ bool path_cells(const PathArgs<T>& a, int64_t i, T* r0, T* r1) {
+    T s[NDIM], e[NDIM];
+#pragma unroll
+    for (int d = 0; d < NDIM; ++d) {
+        s[d] = a.start[d * a.start_stride + i];
+        e[d] = a.end[d * a.end_stride + i];
+    }
+    return path_cells_of<T, NDIM, WHITNEY>(a.g, s, e, r0, r1);
 }
 
 // edges += the box of a sink (its non-zero entries), with global atomics.
@@ -716,8 +787,12 @@ __global__ void __launch_bounds__(256) deposit_paths_tiled_kernel(const PathArgs
 // their atomic adds spread over the L2 (a grid-stride walk keeps every CTA in one small
 // region of a sorted store). Lane l of warp w takes the path l * (BLOCK / 32) + w of
 // the BLOCK: the lanes of a warp are BLOCK / 32 paths apart, in different cells, so the
-// adds of one instruction do not pile onto the same edges.
-template <typename T, int NDIM, int P, bool WHITNEY, int BLOCK = 256, int MINB = 1>
+// adds of one instruction do not pile onto the same edges. The spline paths go piece by
+// piece: a lane whose path is done takes its next one while the others deposit their
+// next piece, so the lanes of a warp deposit pieces together whatever the number of
+// pieces of their paths (a loop over paths would hold every lane until the warp's
+// longest path is done).
+template <typename T, int NDIM, int P, bool WHITNEY, int BLOCK = 256, int MINB = 1, bool FLAT = true>
 __global__ void __launch_bounds__(BLOCK, MINB) deposit_paths_kernel(const PathArgs<T> a) {
     GlobalEdgeSink<T, NDIM> sink;
     sink.edges = a.edges_out;
@@ -726,13 +801,44 @@ __global__ void __launch_bounds__(BLOCK, MINB) deposit_paths_kernel(const PathAr
     const int slot = (threadIdx.x & 31) * (BLOCK / 32) + (threadIdx.x >> 5);
     const int64_t per = ((a.n + gridDim.x - 1) / gridDim.x + BLOCK - 1) / BLOCK * BLOCK;
     const int64_t mine_end = min(a.n, (int64_t)(blockIdx.x + 1) * per);
-    for (int64_t i = (int64_t)blockIdx.x * per + slot; i < mine_end; i += BLOCK) {
-        const T q = a.charges[i];
-        if (q == T(0)) continue;
-        T r0[NDIM], r1[NDIM];
-        if (!path_cells<T, NDIM, WHITNEY>(a, i, r0, r1)) continue;
-        if constexpr (WHITNEY) whitney_path<T, NDIM>(q, r0, r1, a.g, sink);
-        else spline_path<T, NDIM, P>(q, r0, r1, a.g, sink);
+    int64_t i = (int64_t)blockIdx.x * per + slot;
+    if constexpr (!WHITNEY && FLAT) {
+        const bool clamped = any_clamped<T, NDIM>(a.g);
+        SplineWalk<T, NDIM, P> walk;
+        walk.live = false;
+        T q = T(0);
+        int64_t ip = 0;  // the walk's path
+        for (;;) {
+            if (!walk.live) {  // this lane's next path
+                if (i >= mine_end) break;
+                ip = i;
+                i += BLOCK;
+                q = a.charges[ip];
+                T r0[NDIM], r1[NDIM];
+                if (q == T(0) || !path_cells<T, NDIM, false>(a, ip, r0, r1)) continue;
+                walk.begin(r0, r1, a.g);
+            }
+            T p0[NDIM], step[NDIM];
+            if (walk.piece(a.g, p0, step)) spline_piece<T, NDIM, P>(q, p0, step, a.g, clamped, sink);
+            if (walk.ended) {
+                if (walk.more()) {  // a path of several stretches: its ends again
+                    T r0[NDIM], r1[NDIM];
+                    path_cells<T, NDIM, false>(a, ip, r0, r1);
+                    walk.next(r0, r1, a.g);
+                } else {
+                    walk.live = false;
+                }
+            }
+        }
+    } else {
+        for (; i < mine_end; i += BLOCK) {
+            const T q = a.charges[i];
+            if (q == T(0)) continue;
+            T r0[NDIM], r1[NDIM];
+            if (!path_cells<T, NDIM, WHITNEY>(a, i, r0, r1)) continue;
+            if constexpr (WHITNEY) whitney_path<T, NDIM>(q, r0, r1, a.g, sink);
+            else spline_path<T, NDIM, P>(q, r0, r1, a.g, sink);
+        }
     }
 }
 
