@@ -248,6 +248,19 @@ MPF_API int mpf_halo_fold(void* field, int ndim, const int32_t* stored, int64_t 
                   const int32_t* periodic, int dtype, void* stream);
 
 /*
+ * The face slabs of a halo exchange between ranks that each hold a block of a split field
+ * (mpiarray's update_halos / accumulate_halos across processes, behind Field.fill_halos /
+ * Field.exchange_halos, src/mpifield/field.py:601-630). pack copies the `halo` layers
+ * [first, first + halo) along `axis` of the storage (all of the other axes, halos
+ * included, and every component) into `buffer`, contiguous as [outer][halo][inner];
+ * unpack writes the buffer into those layers, or adds it with `accumulate`.
+ */
+MPF_API int mpf_halo_pack(const void* field, int ndim, const int32_t* stored, int64_t ncomp, int32_t halo,
+                  int axis, int32_t first, void* buffer, int dtype, void* stream);
+MPF_API int mpf_halo_unpack(void* field, int ndim, const int32_t* stored, int64_t ncomp, int32_t halo,
+                    int axis, int32_t first, const void* buffer, int accumulate, int dtype, void* stream);
+
+/*
  * dst += deposit / node volume over a block of `num` owned nodes stored with `halo`
  * halo layers per axis (both arrays with the same storage), the volume being
  * prod(cell), halved on the first and last node of a bounded axis. Halo nodes of dst

@@ -79,6 +79,8 @@ _SIGNATURES = {
     "mpf_gather_edges": ([_I, _I, _I, _P, _L, _L, _P, _P, _L, _P, _P, _P, _P, _I, _P], _I),
     "mpf_halo_fill": ([_P, _I, _P, _L, C.c_int32, _P, _I, _P], _I),
     "mpf_halo_fold": ([_P, _I, _P, _L, C.c_int32, _P, _I, _P], _I),
+    "mpf_halo_pack": ([_P, _I, _P, _L, C.c_int32, _I, C.c_int32, _P, _I, _P], _I),
+    "mpf_halo_unpack": ([_P, _I, _P, _L, C.c_int32, _I, C.c_int32, _P, _I, _I, _P], _I),
     "mpf_add_density": ([_P, _P, _I, _P, C.c_int32, _L, _P, _P, _I, _P], _I),
     "mpf_num_tiles": ([_I, _I, _I, _P, _P, _P, _P], _I),
     "mpf_sort_workspace_bytes": ([_L, _L, _P], _I),

@@ -545,6 +545,34 @@ int mpf_halo_fold(void* field, int ndim, const int32_t* stored, int64_t ncomp, i
     return halo_fold(field, ndim, stored, ncomp, halo, periodic, dtype, static_cast<cudaStream_t>(stream));
 }
 
+// The storage, axis and slab [first, first + halo) of a halo pack or unpack, checked.
+static int check_slab(const void* field, const void* buffer, int ndim, const int32_t* stored, int64_t ncomp,
+                      int32_t halo, int axis, int32_t first, int dtype) {
+    if (ndim < 1 || ndim > 3 || !stored || ncomp < 1 || halo < 1) return MPF_ERR_ARGUMENT;
+    if (dtype != MPF_F64 && dtype != MPF_F32) return MPF_ERR_ARGUMENT;
+    if (axis < 0 || axis >= ndim) return MPF_ERR_ARGUMENT;
+    for (int d = 0; d < ndim; ++d)
+        if (stored[d] < 1) return MPF_ERR_SHAPE;
+    if (first < 0 || (int64_t)first + halo > stored[axis]) return MPF_ERR_SHAPE;
+    if (!field || !buffer) return MPF_ERR_ARGUMENT;
+    if (!aligned(field, dtype) || !aligned(buffer, dtype)) return MPF_ERR_ALIGNMENT;
+    return MPF_OK;
+}
+
+int mpf_halo_pack(const void* field, int ndim, const int32_t* stored, int64_t ncomp, int32_t halo, int axis,
+                  int32_t first, void* buffer, int dtype, void* stream) {
+    MPF_TRY(check_slab(field, buffer, ndim, stored, ncomp, halo, axis, first, dtype));
+    return halo_slab(const_cast<void*>(field), buffer, ndim, stored, ncomp, halo, axis, first, 0, dtype,
+                     static_cast<cudaStream_t>(stream));
+}
+
+int mpf_halo_unpack(void* field, int ndim, const int32_t* stored, int64_t ncomp, int32_t halo, int axis,
+                    int32_t first, const void* buffer, int accumulate, int dtype, void* stream) {
+    MPF_TRY(check_slab(field, buffer, ndim, stored, ncomp, halo, axis, first, dtype));
+    return halo_slab(field, const_cast<void*>(buffer), ndim, stored, ncomp, halo, axis, first, accumulate ? 2 : 1,
+                     dtype, static_cast<cudaStream_t>(stream));
+}
+
 int mpf_add_density(void* dst, const void* deposit, int ndim, const int32_t* num, int32_t halo, int64_t ncomp,
                     const double* cell, const int32_t* periodic, int dtype, void* stream) {
     MPF_TRY(check_block(dst, ndim, num, ncomp, halo, periodic, dtype, false));

@@ -60,6 +60,37 @@ __global__ void halo_fold_kernel(T* f, AxisView v, int periodic) {
     }
 }
 
+// Layers [first, first + h) along the axis of the storage <-> a contiguous buffer
+// [outer][h][inner]: the face slabs a rank sends to and takes from its neighbours in the
+// halo exchange of a field split over ranks (mpiarray's update_halos and
+// accumulate_halos between processes). Unpack writes, or adds with ADD (a fold: every
+// buffer entry has its own node, so plain adds).
+template <typename T>
+__global__ void halo_pack_kernel(const T* f, T* buf, AxisView v, int64_t first) {
+    const int64_t count = v.outer * v.h * v.inner;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < count;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t in = k % v.inner;
+        const int64_t l = (k / v.inner) % v.h;
+        const int64_t o = k / (v.inner * v.h);
+        buf[k] = f[(o * v.stored + first + l) * v.inner + in];
+    }
+}
+
+template <typename T, bool ADD>
+__global__ void halo_unpack_kernel(T* f, const T* buf, AxisView v, int64_t first) {
+    const int64_t count = v.outer * v.h * v.inner;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < count;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t in = k % v.inner;
+        const int64_t l = (k / v.inner) % v.h;
+        const int64_t o = k / (v.inner * v.h);
+        T* at = f + (o * v.stored + first + l) * v.inner + in;
+        if (ADD) *at += buf[k];
+        else *at = buf[k];
+    }
+}
+
 template <typename T>
 __global__ void add_density_kernel(T* dst, const T* dep, int ndim, int num0, int num1, int num2,
                                    int h, int64_t ncomp, T v0, T v1, T v2, int p0, int p1, int p2) {
@@ -130,6 +161,41 @@ static int run_density(T* dst, const T* dep, int ndim, const int32_t* num, int h
         ndim > 1 ? periodic[1] : 1, ndim > 2 ? periodic[2] : 1);
     count_launches(1);
     return launch_status();
+}
+
+// The view of `axis` of a storage (h layers per slab).
+static AxisView axis_view(int ndim, const int32_t* stored, int64_t ncomp, int h, int axis) {
+    AxisView v;
+    v.outer = 1;
+    for (int d = 0; d < axis; ++d) v.outer *= stored[d];
+    v.inner = ncomp;
+    for (int d = axis + 1; d < ndim; ++d) v.inner *= stored[d];
+    v.stored = stored[axis];
+    v.owned = stored[axis] - 2 * (int64_t)h;
+    v.h = h;
+    return v;
+}
+
+template <typename T>
+static int run_slab(T* f, T* buf, int ndim, const int32_t* stored, int64_t ncomp, int h, int axis, int first,
+                    int mode, cudaStream_t stream) {
+    const AxisView v = axis_view(ndim, stored, ncomp, h, axis);
+    const int64_t count = v.outer * h * v.inner;
+    if (count == 0) return MPF_OK;
+    const int block = 256;
+    const int64_t blocks = std::min<int64_t>((count + block - 1) / block, (int64_t)sm_count() * 16);
+    if (mode == 0) halo_pack_kernel<T><<<(unsigned)blocks, block, 0, stream>>>(f, buf, v, first);
+    else if (mode == 1) halo_unpack_kernel<T, false><<<(unsigned)blocks, block, 0, stream>>>(f, buf, v, first);
+    else halo_unpack_kernel<T, true><<<(unsigned)blocks, block, 0, stream>>>(f, buf, v, first);
+    count_launches(1);
+    return launch_status();
+}
+
+int halo_slab(void* f, void* buf, int ndim, const int32_t* stored, int64_t ncomp, int h, int axis, int first,
+              int mode, int dtype, cudaStream_t stream) {
+    if (dtype == MPF_F64)
+        return run_slab<double>((double*)f, (double*)buf, ndim, stored, ncomp, h, axis, first, mode, stream);
+    return run_slab<float>((float*)f, (float*)buf, ndim, stored, ncomp, h, axis, first, mode, stream);
 }
 
 int halo_fill(void* f, int ndim, const int32_t* stored, int64_t ncomp, int h, const int32_t* periodic,

@@ -109,6 +109,10 @@ int launch_deposit_paths(int kind, int degree, int ndim, PathArgs<T> a, const Tu
 template <typename T>
 int launch_gather_edges(int kind, int degree, int ndim, const PathArgs<T>& a, cudaStream_t stream);
 
+// Pack (mode 0) the layers [first, first + h) along `axis` into buf, unpack buf into them
+// (mode 1) or add buf onto them (mode 2).
+int halo_slab(void* f, void* buf, int ndim, const int32_t* stored, int64_t ncomp, int h, int axis, int first,
+              int mode, int dtype, cudaStream_t stream);
 int halo_fill(void* f, int ndim, const int32_t* stored, int64_t ncomp, int h, const int32_t* periodic,
               int dtype, cudaStream_t stream);
 int halo_fold(void* f, int ndim, const int32_t* stored, int64_t ncomp, int h, const int32_t* periodic,

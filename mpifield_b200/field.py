@@ -71,6 +71,9 @@ class Field:
         h = self.num_ghost_points
         shape = tuple(m + 2 * h for m in self.num_gridpoints) + (self.num_components,)
         self.local_with_halos = torch.zeros(shape, dtype=dtype, device=self.device)
+        # a field split over ranks: its block's halo exchange (mpifield_b200.exchange), which
+        # fill_halos / exchange_halos then run instead of the one-process kernels
+        self.exchange = None
 
     # ------------------------------------------------------------------ storage --
 
@@ -240,11 +243,18 @@ class Field:
         _lib.check(status, name)
 
     def fill_halos(self) -> None:
-        """Fill the halo layers of periodic axes from the wrapped owned nodes (update_halos)."""
+        """Fill the halo layers of periodic axes from the wrapped owned nodes (update_halos);
+        for a field split over ranks, from the neighbours' owned nodes."""
+        if self.exchange is not None:
+            self.exchange.fill(self.local_with_halos)
+            return
         self._halo_call("mpf_halo_fill")
 
     def exchange_halos(self) -> None:
         """Add the halo layers onto their wrapped owners and clear them (accumulate_halos)."""
+        if self.exchange is not None:
+            self.exchange.fold(self.local_with_halos)
+            return
         self._halo_call("mpf_halo_fold")
 
     def __repr__(self) -> str:

@@ -80,6 +80,12 @@ def test_invalid_arguments_return_a_status_before_any_device_work():
     stored = (C.c_int32 * 1)(3)
     per = (C.c_int32 * 1)(1)
     assert lib.mpf_halo_fold(fake, 1, stored, 1, 2, per, 0, None) == _lib.ERR_SHAPE
+    # halo slabs: an axis outside the block, a slab past the storage, a misaligned buffer
+    s2 = (C.c_int32 * 2)(6, 5)
+    assert lib.mpf_halo_pack(fake, 2, s2, 1, 2, 2, 0, fake, 0, None) == _lib.ERR_ARGUMENT
+    assert lib.mpf_halo_pack(fake, 2, s2, 1, 2, 1, 4, fake, 0, None) == _lib.ERR_SHAPE
+    assert lib.mpf_halo_unpack(fake, 2, s2, 1, 2, 0, 0, fake + 4, 1, 0, None) == _lib.ERR_ALIGNMENT
+    assert lib.mpf_halo_unpack(fake, 2, s2, 1, 0, 0, 0, fake, 1, 0, None) == _lib.ERR_ARGUMENT
     # the deterministic scatter: a workspace too small, misaligned
     size = C.c_size_t()
     assert lib.mpf_scatter_deterministic_workspace_bytes(8 * 8 * 8, C.byref(size)) == 0

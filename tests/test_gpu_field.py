@@ -161,3 +161,44 @@ def test_position_gradient_matches_the_oracle_and_finite_differences(kind, degre
             dn = O.gather(kind, degree, pos - step, field, geom)
             fd = ((up - dn) * values).sum(0) / (2 * eps * cell[d])
             np.testing.assert_allclose(grad[d, inside], fd[inside], rtol=1e-5, atol=1e-5 * np.abs(fd).max())
+
+
+@pytest.mark.parametrize("ndim", [1, 2, 3])
+@pytest.mark.parametrize("halo", [1, 2])
+def test_halo_slabs_and_the_one_rank_exchange(ndim, halo):
+    """mpf_halo_pack / mpf_halo_unpack against tensor slicing, and the halo exchange of a
+    field split over one rank against the one-process mpf_halo_fill / mpf_halo_fold."""
+    from mpifield_b200.exchange import Decomposition, HaloExchange, kernel_pack, kernel_unpack
+
+    rng = np.random.default_rng(ndim * 10 + halo)
+    num = (9, 6, 5)[:ndim]
+    stored = tuple(m + 2 * halo for m in num)
+    for dtype in (torch.float64, torch.float32):
+        t = torch.tensor(rng.normal(size=(*stored, 3)), dtype=dtype, device="cuda")
+        for axis in range(ndim):
+            for first in (0, halo, stored[axis] - halo):
+                buf = torch.empty(t.numel() // stored[axis] * halo, dtype=dtype, device="cuda")
+                kernel_pack(t, halo, axis, first, buf)
+                assert torch.equal(buf, t.narrow(axis, first, halo).reshape(-1))
+                before = t.clone()
+                kernel_unpack(t, halo, axis, first, buf * 2, True)
+                expected = before.clone()
+                expected.narrow(axis, first, halo).mul_(3)
+                torch.testing.assert_close(t, expected, rtol=1e-6, atol=1e-6)
+                kernel_unpack(t, halo, axis, first, buf, False)
+                assert torch.equal(t.narrow(axis, first, halo).reshape(-1), buf)
+    for periodic in ((True,) * ndim, tuple(a % 2 == 0 for a in range(ndim))):
+        ex = HaloExchange(Decomposition(num, periodic, (1,) * ndim, 0), halo)
+        f = mf.Field(ndim, [0.0] * ndim, [1.0] * ndim, num, 3, periodic=periodic, num_ghost_points=halo,
+                     device="cuda")
+        data = torch.tensor(rng.normal(size=(*stored, 3)), device="cuda")
+        f.local_with_halos.copy_(data)
+        mine = data.clone()
+        f.fill_halos()
+        ex.fill(mine)
+        assert torch.equal(mine, f.local_with_halos)
+        f.local_with_halos.copy_(data)
+        mine = data.clone()
+        f.exchange_halos()
+        ex.fold(mine)
+        torch.testing.assert_close(mine, f.local_with_halos, rtol=0, atol=1e-13)
