@@ -696,7 +696,6 @@ __device__ __forceinline__ void cp_async(void* dst, const void* src) {
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 
 // The segment scatter of one component (stencils of at most 27 points). A chunk is
 // 256 x K consecutive markers; thread t owns the K markers t K .. t K + K - 1, which sit in
