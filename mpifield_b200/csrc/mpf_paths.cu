@@ -10,21 +10,62 @@ namespace mpf {
 // faster than shared-memory boxes here, where many lanes add to the same nodes),
 // or the tiled kernel (path 2, staged): chunks of 256 x t.block paths (8 when t.block is
 // 0), a box of edges in t.smem_bytes (96 KB when 0) of shared memory.
+// Edge fields of at most this many entries are deposited through private copies in shared
+// memory when the paths number at least kPrivatePaths per entry (5e6 paths: 1D on 64 or 256
+// nodes 0.28-0.36 ms against 1.1-5.1 ms through the L2; 2D 40 x 50 1.1 / 3.5 ms against
+// 2.5 / 5.1 ms at degree 2 / 3; 3D 12^3 3.9 against 10.7 ms at degree 2).
+constexpr int kPrivateEntries = 8192;
+constexpr int kPrivatePaths = 16;
+
+template <typename T, int NDIM, int P, bool WHITNEY>
+static int run_deposit_private(const PathArgs<T>& a, int64_t entries, cudaStream_t stream) {
+    const int smem = (int)(entries * (int64_t)sizeof(T));
+    // the launch shapes of the direct kernel, as many CTAs per SM as the copies also allow
+    constexpr bool cubic = !WHITNEY && P >= 3;
+    constexpr int threads = cubic ? 128 : 256;
+    auto kernel = cubic ? deposit_paths_private_kernel<T, NDIM, P, WHITNEY, 128, 4>
+                        : deposit_paths_private_kernel<T, NDIM, P, WHITNEY, 256, 2>;
+    const int per_sm = std::max(1, std::min(cubic ? 4 : 2, (228 * 1024) / (smem + 1024)));
+    static int cache[64] = {0};
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= 64) device = 0;
+    if (cache[device] < smem) {
+        if (record_cuda_error(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != MPF_OK)
+            return MPF_ERR_CUDA;
+        cache[device] = smem;
+    }
+    const int64_t blocks = std::min<int64_t>((a.n + threads - 1) / threads, (int64_t)sm_count() * per_sm);
+    kernel<<<(unsigned)std::max<int64_t>(blocks, 1), threads, smem, stream>>>(a);
+    count_launches(1);
+    return launch_status();
+}
+
 template <typename T, int NDIM, int P, bool WHITNEY>
 static int run_deposit(PathArgs<T> a, const Tuning& t, cudaStream_t stream) {
     const int block = 256;
+    // (not the 3D cubic edges: their 144 adds a piece collide in shared memory, and the L2
+    // spreads them better: 19 against 30 ms for 5e6 paths on 12^3)
+    if (t.path == 0 && t.variant != 7 && !(NDIM == 3 && !WHITNEY && P >= 3)) {
+        int64_t entries = NDIM;
+        for (int d = 0; d < NDIM; ++d) entries *= a.g.ext[d];
+        if (entries <= kPrivateEntries && a.n >= kPrivatePaths * entries)
+            return run_deposit_private<T, NDIM, P, WHITNEY>(a, entries, stream);
+    }
     if (t.path != 2) {
         auto launch = [&](auto kernel, int threads) {
             const int64_t blocks = std::min<int64_t>((a.n + threads - 1) / threads, (int64_t)sm_count() * 32);
             kernel<<<(unsigned)std::max<int64_t>(blocks, 1), threads, 0, stream>>>(a);
         };
-        // two CTAs per SM (128 registers a thread) where the path fits them without spills
-        // (WHITNEY and spline edges of degree <= 2: QUADRATIC_EDGES 15% faster than one);
-        // the cubic edges keep one CTA and their registers. Variant 1: one CTA everywhere;
-        // variant 3: spline paths a path at a time instead of piece by piece.
+        // 128 registers a thread: two CTAs of 256 per SM for WHITNEY and the spline edges of
+        // degree <= 2 (no spills; QUADRATIC_EDGES 15% faster than one CTA), four of 128 for
+        // the cubic edges (some spills, but twice the warps of one CTA of 256 at 178
+        // registers: CUBIC_EDGES 137 -> 97 ms at 2^25 paths). Variant 1: one CTA of 256;
+        // variant 3: spline paths a path at a time instead of piece by piece; variant 7:
+        // never through private copies of a small field.
         if constexpr (!WHITNEY && P >= 3) {
             if (t.variant == 3) launch(deposit_paths_kernel<T, NDIM, P, WHITNEY, 256, 1, false>, 256);
-            else launch(deposit_paths_kernel<T, NDIM, P, WHITNEY, 256, 1>, 256);
+            else if (t.variant == 1) launch(deposit_paths_kernel<T, NDIM, P, WHITNEY, 256, 1>, 256);
+            else launch(deposit_paths_kernel<T, NDIM, P, WHITNEY, 128, 4>, 128);
         } else {
             if (t.variant == 1) launch(deposit_paths_kernel<T, NDIM, P, WHITNEY, 256, 1>, 256);
             else if (t.variant == 3) launch(deposit_paths_kernel<T, NDIM, P, WHITNEY, 256, 2, false>, 256);

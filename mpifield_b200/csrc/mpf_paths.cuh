@@ -781,27 +781,13 @@ __global__ void __launch_bounds__(256) deposit_paths_tiled_kernel(const PathArgs
     if (have_box) flush_edge_box<T, NDIM>(tile, a.edges_out, sink, a.g);
 }
 
-// One thread per path, global atomics; BLOCK threads, at least MINB CTAs per SM. Each CTA
-// takes an equal contiguous share of the paths, BLOCK consecutive paths at a time, so that
-// in a store sorted by cell the CTAs work in different regions of the grid at once and
-// their atomic adds spread over the L2 (a grid-stride walk keeps every CTA in one small
-// region of a sorted store). Lane l of warp w takes the path l * (BLOCK / 32) + w of
-// the BLOCK: the lanes of a warp are BLOCK / 32 paths apart, in different cells, so the
-// adds of one instruction do not pile onto the same edges. The spline paths go piece by
-// piece: a lane whose path is done takes its next one while the others deposit their
-// next piece, so the lanes of a warp deposit pieces together whatever the number of
-// pieces of their paths (a loop over paths would hold every lane until the warp's
-// longest path is done).
-template <typename T, int NDIM, int P, bool WHITNEY, int BLOCK = 256, int MINB = 1, bool FLAT = true>
-__global__ void __launch_bounds__(BLOCK, MINB) deposit_paths_kernel(const PathArgs<T> a) {
-    GlobalEdgeSink<T, NDIM> sink;
-    sink.edges = a.edges_out;
-#pragma unroll
-    for (int d = 0; d < 3; ++d) sink.ext[d] = a.g.ext[d];
-    const int slot = (threadIdx.x & 31) * (BLOCK / 32) + (threadIdx.x >> 5);
-    const int64_t per = ((a.n + gridDim.x - 1) / gridDim.x + BLOCK - 1) / BLOCK * BLOCK;
-    const int64_t mine_end = min(a.n, (int64_t)(blockIdx.x + 1) * per);
-    int64_t i = (int64_t)blockIdx.x * per + slot;
+// The paths first, first + STRIDE, ... below end deposited into the sink by one thread.
+// The spline paths go piece by piece: a lane whose path is done takes its next one while
+// the others deposit their next piece, so the lanes of a warp deposit pieces together
+// whatever the number of pieces of their paths (a loop over paths would hold every lane
+// until the warp's longest path is done). FLAT false: a path at a time.
+template <typename T, int NDIM, int P, bool WHITNEY, int STRIDE, bool FLAT, typename Sink>
+__device__ __forceinline__ void deposit_range(const PathArgs<T>& a, int64_t i, int64_t end, const Sink& sink) {
     if constexpr (!WHITNEY && FLAT) {
         const bool clamped = any_clamped<T, NDIM>(a.g);
         SplineWalk<T, NDIM, P> walk;
@@ -810,9 +796,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) deposit_paths_kernel(const PathAr
         int64_t ip = 0;  // the walk's path
         for (;;) {
             if (!walk.live) {  // this lane's next path
-                if (i >= mine_end) break;
+                if (i >= end) break;
                 ip = i;
-                i += BLOCK;
+                i += STRIDE;
                 q = a.charges[ip];
                 T r0[NDIM], r1[NDIM];
                 if (q == T(0) || !path_cells<T, NDIM, false>(a, ip, r0, r1)) continue;
@@ -831,7 +817,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) deposit_paths_kernel(const PathAr
             }
         }
     } else {
-        for (; i < mine_end; i += BLOCK) {
+        for (; i < end; i += STRIDE) {
             const T q = a.charges[i];
             if (q == T(0)) continue;
             T r0[NDIM], r1[NDIM];
@@ -839,6 +825,66 @@ __global__ void __launch_bounds__(BLOCK, MINB) deposit_paths_kernel(const PathAr
             if constexpr (WHITNEY) whitney_path<T, NDIM>(q, r0, r1, a.g, sink);
             else spline_path<T, NDIM, P>(q, r0, r1, a.g, sink);
         }
+    }
+}
+
+// One thread per path, global atomics; BLOCK threads, at least MINB CTAs per SM. Each CTA
+// takes an equal contiguous share of the paths, BLOCK consecutive paths at a time, so that
+// in a store sorted by cell the CTAs work in different regions of the grid at once and
+// their atomic adds spread over the L2 (a grid-stride walk keeps every CTA in one small
+// region of a sorted store). Lane l of warp w takes the path l * (BLOCK / 32) + w of
+// the BLOCK: the lanes of a warp are BLOCK / 32 paths apart, in different cells, so the
+// adds of one instruction do not pile onto the same edges.
+template <typename T, int NDIM, int P, bool WHITNEY, int BLOCK = 256, int MINB = 1, bool FLAT = true>
+__global__ void __launch_bounds__(BLOCK, MINB) deposit_paths_kernel(const PathArgs<T> a) {
+    GlobalEdgeSink<T, NDIM> sink;
+    sink.edges = a.edges_out;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) sink.ext[d] = a.g.ext[d];
+    const int slot = (threadIdx.x & 31) * (BLOCK / 32) + (threadIdx.x >> 5);
+    const int64_t per = ((a.n + gridDim.x - 1) / gridDim.x + BLOCK - 1) / BLOCK * BLOCK;
+    const int64_t mine_end = min(a.n, (int64_t)(blockIdx.x + 1) * per);
+    deposit_range<T, NDIM, P, WHITNEY, BLOCK, FLAT>(a, (int64_t)blockIdx.x * per + slot, mine_end, sink);
+}
+
+// Adds v to edge (node per axis, axis) of a private copy of the whole edge field in
+// shared memory (same layout as the field).
+template <typename T, int NDIM> struct SharedEdgeSink {
+    T* box;
+    int ext[3];
+    __device__ __forceinline__ void add(const int* node, int axis, T v) const {
+        int k = node[0];
+#pragma unroll
+        for (int d = 1; d < NDIM; ++d) k = k * ext[d] + node[d];
+        atomicAdd(box + k * NDIM + axis, v);
+    }
+};
+
+// The path deposit onto a small edge field (entries in shared memory): each CTA adds its
+// share of the paths (as deposit_paths_kernel) into a private copy of the whole field in
+// shared memory and then adds the copy's non-zero entries to the field, one global atomic
+// each. On a grid of a few hundred edges the global adds of every CTA would pile onto the
+// same few L2 lines; here they meet only in the CTA's shared memory.
+template <typename T, int NDIM, int P, bool WHITNEY, int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) deposit_paths_private_kernel(const PathArgs<T> a) {
+    SharedEdgeSink<T, NDIM> sink;
+    sink.box = reinterpret_cast<T*>(mpf_dynamic_smem);
+    int total = NDIM;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        sink.ext[d] = a.g.ext[d];
+        if (d < NDIM) total *= a.g.ext[d];
+    }
+    for (int q = threadIdx.x; q < total; q += BLOCK) sink.box[q] = T(0);
+    __syncthreads();
+    const int slot = (threadIdx.x & 31) * (BLOCK / 32) + (threadIdx.x >> 5);
+    const int64_t per = ((a.n + gridDim.x - 1) / gridDim.x + BLOCK - 1) / BLOCK * BLOCK;
+    const int64_t mine_end = min(a.n, (int64_t)(blockIdx.x + 1) * per);
+    deposit_range<T, NDIM, P, WHITNEY, BLOCK, true>(a, (int64_t)blockIdx.x * per + slot, mine_end, sink);
+    __syncthreads();
+    for (int q = threadIdx.x; q < total; q += BLOCK) {
+        const T v = sink.box[q];
+        if (v != T(0)) atomicAdd(a.edges_out + q, v);
     }
 }
 

@@ -168,3 +168,36 @@ def test_full_size_continuity_128_cubed(degree):
     div = ew.divergence_block(edges, grid)
     change = (after - before)[..., 0]
     assert float((div - change).abs().max()) < 1e-10 * max(1.0, float(change.abs().max()))
+
+
+@pytest.mark.parametrize("ndim", [1, 2, 3])
+@pytest.mark.parametrize("degree", [1, 2, 3])
+def test_small_fields_through_private_copies_match_the_oracle(ndim, degree):
+    """Edge fields of a few hundred entries with many paths: each CTA deposits into a
+    private copy in shared memory (the default there) -- the same as the oracle and as the
+    global-atomic kernel (variant 7), for every boundary code."""
+    rng = np.random.default_rng(300 + 10 * ndim + degree)
+    shape = {1: (24,), 2: (12, 10), 3: (7, 6, 5)}[ndim]
+    for codes in ((1,) * ndim, (0,) * ndim, (2,) + (1,) * (ndim - 1)):
+        if 2 in codes and degree == 1:
+            continue
+        lower = rng.uniform(-1, 1, ndim)
+        cell = rng.uniform(0.2, 0.6, ndim)
+        upper = lower + cell * (np.array(shape) - 1)
+        n = 40_000
+        start = rng.uniform(lower - cell, upper + cell, (n, ndim)).T.copy()
+        end = start + rng.normal(scale=1.5 * cell[:, None], size=start.shape)
+        charges = rng.normal(size=n)
+        charges[::13] = 0.0
+        geom = (*lower, *cell, *shape, *codes)
+        ext = tuple(s + (degree - 1 if c == 2 else 0) for s, c in zip(shape, codes))
+        expected = O.deposit_spline(degree, start, end, charges, np.zeros((*ext, ndim)), geom)
+        got = run_deposit(_lib.SPLINE, degree, start, end, charges, (*ext, ndim), geom)
+        np.testing.assert_allclose(got, expected, rtol=0, atol=1e-12 * np.abs(expected).max())
+        edges = torch.zeros((*ext, ndim), dtype=torch.float64, device=DEV)
+        deposit_paths(_lib.SPLINE, degree, cu(start), cu(end), cu(charges), edges, geom, _lib.tuning_struct(variant=7))
+        np.testing.assert_allclose(edges.cpu().numpy(), expected, rtol=0, atol=1e-12 * np.abs(expected).max())
+        if degree == 1 and 2 not in codes:
+            exp_w = O.deposit_whitney(start, end, charges, np.zeros((*ext, ndim)), geom)
+            got = run_deposit(_lib.LINEAR, 1, start, end, charges, (*ext, ndim), geom)
+            np.testing.assert_allclose(got, exp_w, rtol=0, atol=1e-12 * np.abs(exp_w).max())
