@@ -56,8 +56,10 @@ static int run_deposit(PathArgs<T> a, const Tuning& t, cudaStream_t stream) {
             const int64_t blocks = std::min<int64_t>((a.n + threads - 1) / threads, (int64_t)sm_count() * 32);
             kernel<<<(unsigned)std::max<int64_t>(blocks, 1), threads, 0, stream>>>(a);
         };
-        // 128 registers a thread: two CTAs of 256 per SM for WHITNEY and the spline edges of
-        // degree <= 2 (no spills; QUADRATIC_EDGES 15% faster than one CTA), four of 128 for
+        // WHITNEY: five CTAs of 128 per SM (96 registers; 4% faster than two of 256 on a
+        // sorted store). 128 registers a thread: two CTAs of 256 per SM for the spline edges
+        // of degree <= 2 (no spills; QUADRATIC_EDGES 15% faster than one CTA; 96 or 80
+        // registers spill and measured 15-25% slower), four of 128 for
         // the cubic edges (some spills, but twice the warps of one CTA of 256 at 178
         // registers: CUBIC_EDGES 137 -> 97 ms at 2^25 paths). Variant 1: one CTA of 256;
         // variant 3: spline paths a path at a time instead of piece by piece; variant 7:
@@ -69,6 +71,7 @@ static int run_deposit(PathArgs<T> a, const Tuning& t, cudaStream_t stream) {
         } else {
             if (t.variant == 1) launch(deposit_paths_kernel<T, NDIM, P, WHITNEY, 256, 1>, 256);
             else if (t.variant == 3) launch(deposit_paths_kernel<T, NDIM, P, WHITNEY, 256, 2, false>, 256);
+            else if constexpr (WHITNEY) launch(deposit_paths_kernel<T, NDIM, P, WHITNEY, 128, 5>, 128);
             else launch(deposit_paths_kernel<T, NDIM, P, WHITNEY, 256, 2>, 256);
         }
         count_launches(1);
