@@ -69,6 +69,8 @@ def parse() -> argparse.Namespace:
     p.add_argument("--serve-requests", type=int, default=10000, help="requests of the serving stream (0: skip)")
     p.add_argument("--paths-only", type=int, default=0, metavar="N",
                    help="measure only the path deposits, at N paths on 128^3 (a profiling case)")
+    p.add_argument("--autograd-only", action="store_true",
+                   help="measure only the differentiation step (512^2 cubic, 2^22 markers; a profiling case)")
     p.add_argument("--serve-rate", type=float, default=20000.0,
                    help="Poisson arrival rate of the stream, per s (the default outruns both arms: capacity)")
     p.add_argument("--serve-latency-rate", type=float, default=1500.0,
@@ -1012,6 +1014,13 @@ def main() -> None:
                 peak, _ = read_peak()
                 print(json.dumps({"path_deposit": measure_paths(device, max(1, args.steps), peak, args.paths_only,
                                                                 cpu_sample=None)}))
+            return
+        if args.autograd_only:
+            device = torch.device("cuda", local)
+            torch.cuda.set_device(device)
+            if rank == 0:
+                peak, _ = read_peak()
+                print(json.dumps({"autograd": measure_autograd(device, max(1, args.steps), peak)}))
             return
         if args.impl == "reference":
             run_reference(args, world, rank)
