@@ -399,6 +399,8 @@ MPF_API int mpf_unpermute_rows(void* dst, int64_t dst_stride, const void* src, i
  */
 #define MPF_OP_GATHER 0
 #define MPF_OP_SCATTER 1
+#define MPF_OP_PATHS 2 /* path deposit: positions = start, field = end (rows out_stride apart),
+                          values = charges (n,), out = the edge field added into */
 
 typedef struct mpf_batch_request {
     int32_t op, kind, degree, ndim;
@@ -430,9 +432,12 @@ typedef struct mpf_batch_header {
 MPF_API int64_t mpf_batch_request_size(void);
 
 /*
- * Checks one request as mpf_gather / mpf_scatter would and fills *r (host memory) for
- * the table; first_tile is left for the caller. op MPF_OP_GATHER: values ignored, out is
- * the result; MPF_OP_SCATTER: field ignored, out is the field added into.
+ * Checks one request as mpf_gather / mpf_scatter / mpf_deposit_paths would and fills *r
+ * (host memory) for the table; first_tile is left for the caller. op MPF_OP_GATHER: values
+ * ignored, out is the result; MPF_OP_SCATTER: field ignored, out is the field added into;
+ * MPF_OP_PATHS (kind MPF_LINEAR degree 1 WHITNEY, MPF_SPLINE degree 1-3 spline edges):
+ * positions the starts, field the ends (rows out_stride apart), values the n charges, out
+ * the edge field extent + (ndim,) added into, ncomp ignored.
  */
 MPF_API int mpf_batch_request_init(mpf_batch_request* r, int op, int kind, int degree, int ndim,
                                    const void* positions, int64_t pos_stride, const void* values,

@@ -59,7 +59,7 @@ class BatchHeader(C.Structure):
                 ("next_tile", C.c_int64), ("finished", C.c_int64), ("pad", C.c_int64 * 3)]
 
 
-OP_GATHER, OP_SCATTER = 0, 1
+OP_GATHER, OP_SCATTER, OP_PATHS = 0, 1, 2
 
 _P = C.c_void_p
 _I = C.c_int

@@ -1,14 +1,16 @@
-// mpf_batch.cu -- the serving batch: many small FP64 gathers and scatters in one launch.
+// mpf_batch.cu -- the serving batch: many small FP64 gathers, scatters and path deposits in
+// one launch.
 //
 // The requests of a batch sit in a device table (mpf_batch_request); request r owns the
 // tiles first_tile .. first_tile + ceil(n / tile_markers) - 1. Persistent CTAs take tiles
 // from the header's counter; a tile is a range of one request's markers, one marker per
-// thread, with the arithmetic of the single-request kernels (the same stencils, global
-// loads, FP64 atomic adds for the scatter). The last CTA to finish resets the counter, so
+// thread (a path per thread for a deposit), with the arithmetic of the single-request
+// kernels (the same stencils and path walks, global loads, FP64 atomic adds for the
+// scatter and the deposit). The last CTA to finish resets the counter, so
 // the launch replays from a CUDA graph with nothing but the table rewritten.
 #include <algorithm>
 
-#include "mpf_nodes.cuh"
+#include "mpf_paths.cuh"
 #include "mpifield_b200.h"
 
 namespace mpf {
@@ -84,8 +86,39 @@ __device__ __noinline__ void batch_scatter(const mpf_batch_request& r, int64_t f
     }
 }
 
+// Paths first .. last - 1 of a deposit request (WHITNEY or spline edges of degree P).
+template <int NDIM, int P, bool WHITNEY>
+__device__ __noinline__ void batch_paths(const mpf_batch_request& r, int64_t first, int64_t last) {
+    PathArgs<double> a{};
+    a.g = grid_of(r);
+    a.start = r.positions;
+    a.start_stride = r.pos_stride;
+    a.end = r.field;
+    a.end_stride = r.out_stride;
+    a.charges = r.values;
+    a.edges_out = r.out;
+    a.n = r.n;
+    GlobalEdgeSink<double, NDIM> sink;
+    sink.edges = r.out;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) sink.ext[d] = a.g.ext[d];
+    for (int64_t i = first + threadIdx.x; i < last; i += blockDim.x) {
+        const double q = r.values[i];
+        if (q == 0.0) continue;
+        double r0[NDIM], r1[NDIM];
+        if (!path_cells<double, NDIM, WHITNEY>(a, i, r0, r1)) continue;
+        if constexpr (WHITNEY) whitney_path<double, NDIM>(q, r0, r1, a.g, sink);
+        else spline_path<double, NDIM, P>(q, r0, r1, a.g, sink);
+    }
+}
+
 template <int NDIM, int KIND, int P>
 __device__ __forceinline__ void batch_op(const mpf_batch_request& r, int64_t first, int64_t last) {
+    if (r.op == MPF_OP_PATHS) {
+        if constexpr (KIND == LINEAR) batch_paths<NDIM, 1, true>(r, first, last);
+        else if constexpr (KIND == SPLINE && P >= 1) batch_paths<NDIM, P, false>(r, first, last);
+        return;
+    }
     if (r.op == MPF_OP_GATHER) batch_gather<NDIM, KIND, P>(r, first, last);
     else batch_scatter<NDIM, KIND, P>(r, first, last);
 }

@@ -456,18 +456,27 @@ static bool valid_edge_kind(int kind, int degree) {
     return false;
 }
 
-int mpf_deposit_paths(int kind, int degree, int ndim, const void* start, int64_t start_stride, const void* end,
-                      int64_t end_stride, const void* charges, int64_t n, void* edges, const double* lower,
-                      const double* cell, const int32_t* num, const int32_t* code, int dtype,
-                      const mpf_tuning* tuning, void* stream) {
-    const Tuning t = tuning_of(tuning);
+// The arguments of a path deposit: kind and degree, grid, and the rows of starts, ends and
+// charges (strides of 0 taken as n).
+static int check_paths(int kind, int degree, int ndim, const void* start, int64_t& start_stride, const void* end,
+                       int64_t& end_stride, const void* charges, int64_t n, const double* lower, const double* cell,
+                       const int32_t* num, const int32_t* code, int dtype) {
     if (!valid_edge_kind(kind, degree) || (dtype != MPF_F64 && dtype != MPF_F32)) return MPF_ERR_ARGUMENT;
     MPF_TRY(check_grid(kind == MPF_LINEAR ? MPF_LINEAR : MPF_SPLINE, degree, ndim, lower, cell, num, code));
     if (n < 0) return MPF_ERR_ARGUMENT;
     MPF_TRY(check_rows(start, start_stride, n, ndim, dtype));
     MPF_TRY(check_rows(end, end_stride, n, ndim, dtype));
     int64_t one = n;
-    MPF_TRY(check_rows(charges, one, n, 1, dtype));
+    return check_rows(charges, one, n, 1, dtype);
+}
+
+int mpf_deposit_paths(int kind, int degree, int ndim, const void* start, int64_t start_stride, const void* end,
+                      int64_t end_stride, const void* charges, int64_t n, void* edges, const double* lower,
+                      const double* cell, const int32_t* num, const int32_t* code, int dtype,
+                      const mpf_tuning* tuning, void* stream) {
+    const Tuning t = tuning_of(tuning);
+    MPF_TRY(check_paths(kind, degree, ndim, start, start_stride, end, end_stride, charges, n, lower, cell, num, code,
+                        dtype));
     if (n == 0) return MPF_OK;
     if (!edges) return MPF_ERR_ARGUMENT;
     if (!aligned(edges, dtype)) return MPF_ERR_ALIGNMENT;
@@ -747,13 +756,21 @@ int mpf_batch_request_init(mpf_batch_request* r, int op, int kind, int degree, i
                            void* out, int64_t out_stride, int ncomp, const double* lower, const double* cell,
                            const int32_t* num, const int32_t* code) {
     if (!r) return MPF_ERR_ARGUMENT;
-    if (op != MPF_OP_GATHER && op != MPF_OP_SCATTER) return MPF_ERR_ARGUMENT;
-    if (!valid_kind(kind, degree)) return MPF_ERR_ARGUMENT;
-    MPF_TRY(check_grid(kind, degree, ndim, lower, cell, num, code));
-    if (n < 0 || ncomp < 1) return MPF_ERR_ARGUMENT;
-    MPF_TRY(check_rows(positions, pos_stride, n, ndim, MPF_F64));
+    if (op != MPF_OP_GATHER && op != MPF_OP_SCATTER && op != MPF_OP_PATHS) return MPF_ERR_ARGUMENT;
+    if (op == MPF_OP_PATHS) {
+        MPF_TRY(check_paths(kind, degree, ndim, positions, pos_stride, field, out_stride, values, n, lower, cell, num,
+                            code, MPF_F64));
+        ncomp = ndim;
+    } else {
+        if (!valid_kind(kind, degree)) return MPF_ERR_ARGUMENT;
+        MPF_TRY(check_grid(kind, degree, ndim, lower, cell, num, code));
+        if (n < 0 || ncomp < 1) return MPF_ERR_ARGUMENT;
+        MPF_TRY(check_rows(positions, pos_stride, n, ndim, MPF_F64));
+    }
     if (!out || !aligned(out, MPF_F64)) return out ? MPF_ERR_ALIGNMENT : MPF_ERR_ARGUMENT;
-    if (op == MPF_OP_GATHER) {
+    if (op == MPF_OP_PATHS) {
+        // (checked above)
+    } else if (op == MPF_OP_GATHER) {
         if (!field) return MPF_ERR_ARGUMENT;
         if (!aligned(field, MPF_F64)) return MPF_ERR_ALIGNMENT;
         MPF_TRY(check_rows(out, out_stride, n, ncomp, MPF_F64));

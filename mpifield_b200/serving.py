@@ -8,9 +8,9 @@ count, degree, operation), and:
   field and its outputs stay resident until it completes), in arrival order;
 - runs a large gather or scatter on its markers sorted by cell tile (the sort once at
   admission, the kernels on the sorted copy, a gather's result returned to the request's
-  marker order), and a path deposit as one launch, each on one stream of a pool, so that
-  the work of several requests overlaps on the device;
-- packs the small gathers and scatters that arrived since the last batch into one
+  marker order), and a large path deposit as one launch, each on one stream of a pool, so
+  that the work of several requests overlaps on the device;
+- packs the small gathers, scatters and path deposits that arrived since the last batch into one
   persistent launch (``mpf_batch_launch``) from a per-request tile table, captured once
   in a CUDA graph and replayed with each new table; the tile size and the CTA count come
   from `autotune_batch`;
@@ -260,7 +260,7 @@ def run(req: Request, b: Buffers) -> torch.Tensor:
 # ------------------------------------------------------------------------ batches --
 
 class BatchRunner:
-    """Small gathers and scatters in one launch from a device table, replayed from a CUDA
+    """Small gathers, scatters and path deposits in one launch from a device table, replayed from a CUDA
     graph: the pinned host table and header are rewritten, then the graph copies them to
     the device and launches ``mpf_batch_launch``."""
 
@@ -305,12 +305,22 @@ class BatchRunner:
         return self.done is not None and not self.done.query()
 
     def fill(self, work: list) -> None:
-        """Writes the table for ``work``: (request, buffers) pairs of small gathers/scatters."""
+        """Writes the table for ``work``: (request, buffers) pairs of small requests."""
         tiles = 0
         lib = _lib.library()
         for i, (req, b) in enumerate(work):
-            kind, degree = NODE_KIND[req.degree]
             lower, cell, num, code, ndim = _lib.geometry_arrays(req.geometry)
+            if req.op == "paths":  # starts, ends (rows n apart), charges, the edge field
+                kind, degree = PATH_KIND[req.degree]
+                status = lib.mpf_batch_request_init(
+                    C.byref(self.entries[i]), _lib.OP_PATHS, kind, degree, ndim, b["positions"].data_ptr(), req.n,
+                    b["values"].data_ptr(), req.n, req.n, b["end"].data_ptr(), b["out"].data_ptr(), req.n, ndim,
+                    lower, cell, num, code)
+                _lib.check(status, "batch_request_init")
+                self.entries[i].first_tile = tiles
+                tiles += -(-req.n // self.tile_markers)
+                continue
+            kind, degree = NODE_KIND[req.degree]
             gather = req.op == "gather"
             status = lib.mpf_batch_request_init(
                 C.byref(self.entries[i]), _lib.OP_GATHER if gather else _lib.OP_SCATTER, kind, degree, ndim,
@@ -349,13 +359,13 @@ _TUNED: dict = {}
 
 def autotune_batch(device, reps: int = 3, seed: int = 3) -> dict:
     """The batch launch's tile size (markers per tile) and CTA count, measured on a
-    synthetic mix of small requests (gathers and scatters of 1-3 dimensions, degrees 1-3,
-    1e3-1e5 markers); the fastest pair is kept for the process."""
+    synthetic mix of small requests (gathers, scatters and path deposits of 1-3 dimensions,
+    degrees 1-3, 1e3-1e5 markers); the fastest pair is kept for the process."""
     key = str(torch.device(device))
     if key in _TUNED:
         return _TUNED[key]
     dev = torch.device(device)
-    reqs = [r for r in make_stream(96, 1e6, seed, markers=(1e3, 1e5)) if r.op != "paths"][:48]
+    reqs = make_stream(48, 1e6, seed, markers=(1e3, 1e5))
     work = [(r, inputs_of(r, dev)) for r in reqs]
     sms = torch.cuda.get_device_properties(dev).multi_processor_count
     best = None
@@ -431,7 +441,7 @@ class Server:
         return self.arena.peak
 
     def _small(self, req: Request) -> bool:
-        return req.op != "paths" and req.n <= self.small_markers
+        return req.n <= self.small_markers
 
     def _admit(self, req: Request) -> _Job | None:
         block = self.arena.alloc(req.nbytes())

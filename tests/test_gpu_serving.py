@@ -21,7 +21,8 @@ DEV = torch.device("cuda")
 
 
 def _small_work(seed, count=40, markers=(1e3, 3e4)):
-    reqs = [r for r in S.make_stream(3 * count, 1e6, seed, markers=markers) if r.op != "paths"][:count]
+    reqs = S.make_stream(count, 1e6, seed, markers=markers)
+    assert {r.op for r in reqs} == {"gather", "scatter", "paths"}
     return [(r, S.inputs_of(r, DEV)) for r in reqs]
 
 
