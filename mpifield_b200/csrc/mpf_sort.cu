@@ -146,21 +146,32 @@ __global__ void scan_chunks_kernel(uint32_t* data, int64_t count, const uint32_t
 
 // The stable scatter of one pass. Warp w of a CTA owns the contiguous segment
 // [w * 32 * kSortItems, (w + 1) * 32 * kSortItems) of the CTA's tile and walks it in
-// rounds of 32 consecutive keys; the per-warp digit counts live in dynamic shared
-// memory (kWarps << BITS words) and become the warps' output offsets in place.
+// rounds of 32 consecutive keys, ranking each key among the warp's keys of its digit
+// (__match_any_sync) against per-warp digit counts in shared memory. The tile's pairs are
+// then placed in shared memory in digit order (a CTA-wide scan of the digit counts) and
+// written out in that order: consecutive threads write consecutive ranks of one digit's
+// run, so the writes of a warp cover a few runs instead of 32 scattered words.
 template <int BITS>
 __global__ void digit_scatter_kernel(const uint32_t* keys_in, const int32_t* vals_in, int64_t n,
                                      const int64_t* n_dev, int shift, const uint32_t* offsets, int64_t nblocks,
                                      uint32_t* keys_out, int32_t* vals_out) {
     constexpr int DIGITS = 1 << BITS;
+    constexpr int PER = DIGITS / kSortBlock;  // digits a thread scans (DIGITS >= kSortBlock)
+    static_assert(DIGITS % kSortBlock == 0, "a whole number of digits per thread");
     if (n_dev) n = min(n, *n_dev);
-    extern __shared__ uint32_t warp_count[];  // [kWarps][DIGITS]
+    extern __shared__ uint32_t smem_words[];
+    uint32_t* warp_count = smem_words;                 // [kWarps][DIGITS]
+    uint32_t* digit_start = warp_count + kWarps * DIGITS;  // [DIGITS]: the tile's first place of a digit
+    uint32_t* tile_keys = digit_start + DIGITS;        // [kSortTile]
+    int32_t* tile_vals = reinterpret_cast<int32_t*>(tile_keys + kSortTile);  // [kSortTile]
+    __shared__ uint32_t warp_sums[kWarps];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     for (int d = threadIdx.x; d < kWarps * DIGITS; d += blockDim.x) warp_count[d] = 0;
     __syncthreads();
     uint32_t* mine = warp_count + warp * DIGITS;
-    const int64_t seg = (int64_t)blockIdx.x * kSortTile + (int64_t)warp * 32 * kSortItems;
+    const int64_t base = (int64_t)blockIdx.x * kSortTile;
+    const int64_t seg = base + (int64_t)warp * 32 * kSortItems;
     uint32_t key[kSortItems];
     int32_t val[kSortItems];
     uint32_t rank[kSortItems];
@@ -182,25 +193,59 @@ __global__ void digit_scatter_kernel(const uint32_t* keys_in, const int32_t* val
         __syncwarp();
     }
     __syncthreads();
-    // every warp's run of a digit starts after the CTA's earlier warps, in the whole array
-    for (int d = threadIdx.x; d < DIGITS; d += blockDim.x) {
-        uint32_t s = offsets[(int64_t)d * nblocks + blockIdx.x];
+    // per digit: the warps' counts become their first places within the digit's run, and
+    // the digit's run in the tile starts after the smaller digits' runs (a CTA-wide scan)
+    uint32_t total[PER];
+    uint32_t run = 0;
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+        const int d = threadIdx.x * PER + q;
+        uint32_t s = 0;
         for (int w = 0; w < kWarps; ++w) {
             const uint32_t c = warp_count[w * DIGITS + d];
             warp_count[w * DIGITS + d] = s;
             s += c;
         }
+        total[q] = s;
+        run += s;
+    }
+    uint32_t incl = run;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t x = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += x;
+    }
+    if (lane == 31) warp_sums[warp] = incl;
+    __syncthreads();
+    uint32_t before_warps = 0;
+    for (int w = 0; w < warp; ++w) before_warps += warp_sums[w];
+    uint32_t at = before_warps + incl - run;
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+        digit_start[threadIdx.x * PER + q] = at;
+        at += total[q];
     }
     __syncthreads();
+    // the tile's pairs in digit order in shared memory
 #pragma unroll
     for (int r = 0; r < kSortItems; ++r) {
         const int64_t i = seg + (int64_t)r * 32 + lane;
         if (i < n) {
             const uint32_t digit = (key[r] >> shift) & (DIGITS - 1);
-            const uint32_t dst = mine[digit] + rank[r];
-            keys_out[dst] = key[r];
-            vals_out[dst] = val[r];
+            const uint32_t place = digit_start[digit] + mine[digit] + rank[r];
+            tile_keys[place] = key[r];
+            tile_vals[place] = val[r];
         }
+    }
+    __syncthreads();
+    // written out in that order: place p of digit d goes to the digit's run of this CTA
+    const int count = (int)min((int64_t)kSortTile, max((int64_t)0, n - base));
+    for (int p = threadIdx.x; p < count; p += blockDim.x) {
+        const uint32_t k = tile_keys[p];
+        const uint32_t digit = (k >> shift) & (DIGITS - 1);
+        const uint32_t dst = offsets[(int64_t)digit * nblocks + blockIdx.x] + (uint32_t)p - digit_start[digit];
+        keys_out[dst] = k;
+        vals_out[dst] = tile_vals[p];
     }
 }
 
@@ -319,7 +364,7 @@ static int radix_pass(const uint32_t* kin, const int32_t* vin, int64_t n, const 
     if (launch_status() != MPF_OK) return MPF_ERR_CUDA;
     const int st = scan_exclusive(counts, nb << BITS, sums, stream);
     if (st != MPF_OK) return st;
-    const int smem = kWarps * (1 << BITS) * (int)sizeof(uint32_t);
+    const int smem = (kWarps * (1 << BITS) + (1 << BITS) + 2 * kSortTile) * (int)sizeof(uint32_t);
     static int configured = 0;
     if (configured < smem) {
         if (record_cuda_error(cudaFuncSetAttribute(digit_scatter_kernel<BITS>,
