@@ -201,3 +201,19 @@ def test_small_fields_through_private_copies_match_the_oracle(ndim, degree):
             exp_w = O.deposit_whitney(start, end, charges, np.zeros((*ext, ndim)), geom)
             got = run_deposit(_lib.LINEAR, 1, start, end, charges, (*ext, ndim), geom)
             np.testing.assert_allclose(got, exp_w, rtol=0, atol=1e-12 * np.abs(exp_w).max())
+
+
+@pytest.mark.parametrize("degree", [1, 2, 3])
+def test_float32_deposits_stay_within_their_bound(degree):
+    """The float32 build of the deposit (the direct kernel on a large field, the private
+    copies on a small one) against the float64 deposit of the float32-rounded paths."""
+    rng = np.random.default_rng(500 + degree)
+    for shape, n in (((40, 36, 32), 200_000), ((6, 5, 4), 60_000)):
+        geom = (0.0, 0.0, 0.0, *(1.0 / s for s in shape), *shape, 1, 1, 1)
+        start = rng.uniform(0, 1, (3, n)).astype(np.float32).astype(np.float64)
+        step = rng.uniform(-0.9, 0.9, (3, n)) / np.array(shape)[:, None]
+        end = (start + step).astype(np.float32).astype(np.float64)
+        charges = rng.uniform(0.5, 1.5, n).astype(np.float32).astype(np.float64)
+        ref = run_deposit(_lib.SPLINE, degree, start, end, charges, (*shape, 3), geom)
+        got = run_deposit(_lib.SPLINE, degree, start, end, charges, (*shape, 3), geom, dtype=torch.float32)
+        assert np.abs(got - ref).max() <= 2e-4 * np.abs(ref).max(), degree
