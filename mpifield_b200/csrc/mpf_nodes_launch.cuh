@@ -54,6 +54,13 @@ template <typename T, int NDIM> static int bulk_positions(const NodeArgs<T>& a) 
     return (p % 16 == 0) && (NDIM == 1 || (a.pos_stride * (int64_t)sizeof(T)) % 16 == 0) ? 1 : 0;
 }
 
+// CTAs per SM of the tile kernels by element type: the float builds hold fewer registers
+// (the float tile scatter fits 80 registers, the lean gather 64, without spills) and half
+// the shared memory, so they run more CTAs (2^26 markers on 256^3: float scatter 1.99 ->
+// 1.52 ms at three CTAs, gather 1.17 -> 1.14 ms at four); the double builds spill there.
+template <typename T> constexpr int kLeanGatherMinBlocks = sizeof(T) == 4 ? 4 : 3;
+template <typename T> constexpr int kTileScatterMinBlocksOf = sizeof(T) == 4 ? 3 : kTileScatterMinBlocks;
+
 // The lean tile gather (mpf_runs.cuh): BLOCK threads, MINB CTAs per SM, BUFFERS boxes.
 // Returns MPF_ERR_ARGUMENT, launching nothing, when the boxes do not fit.
 template <typename T, int NDIM, int KIND, int P, int NC, int BLOCK, int MINB, int BUFFERS>
@@ -86,7 +93,8 @@ static int run_gather_lean(NodeArgs<T> a, cudaStream_t stream) {
 
 // Gather variants for markers sorted by cell tile (periodic axes, 1-3 components, fewer
 // than 2^31 field entries, the tile's box within shared memory): 0 (default) the lean
-// tile gather with one box and three CTAs of 256 per SM, 6 with two boxes and one CTA of
+// tile gather with one box and three (double) or four (float) CTAs of 256 per SM, 6 with
+// two boxes and one CTA of
 // 512. Otherwise, and for unsorted markers: through L1 while the field has fewer than
 // 2^31 entries, else with staged boxes; 1 staged boxes (path 1: global reads in that
 // kernel); 2 through L1.
@@ -96,7 +104,7 @@ static int run_gather(NodeArgs<T> a, const Tuning& t, cudaStream_t stream) {
         if (a.tile_start && (t.variant == 0 || t.variant == 6) && t.path != 1 && all_periodic<T, NDIM>(a) &&
             field_entries<T, NDIM>(a) < ((int64_t)1 << 31)) {
             const int st = t.variant == 6 ? run_gather_lean<T, NDIM, KIND, P, NC, 512, 1, 2>(a, stream)
-                                          : run_gather_lean<T, NDIM, KIND, P, NC, 256, 3, 1>(a, stream);
+                                          : run_gather_lean<T, NDIM, KIND, P, NC, 256, kLeanGatherMinBlocks<T>, 1>(a, stream);
             if (st != MPF_ERR_ARGUMENT) return st;
         }
     }
@@ -251,7 +259,8 @@ static int run_scatter(NodeArgs<T> a, const Tuning& t, cudaStream_t stream) {
                                               : run_scatter_lean<T, NDIM, KIND, P, 256, 2>(a, stream);
                 if (st != MPF_ERR_ARGUMENT) return st;
             }
-            const int st = run_scatter_tiles<T, NDIM, KIND, P, kSegment, kTileScatterMinBlocks, kTileScatterBlock>(a, stream);
+            const int st =
+                run_scatter_tiles<T, NDIM, KIND, P, kSegment, kTileScatterMinBlocksOf<T>, kTileScatterBlock>(a, stream);
             if (st != MPF_ERR_ARGUMENT) return st;
         }
         if (t.variant == 3) return run_scatter_segments<T, NDIM, KIND, P, 4, 3>(a, t, stream);
