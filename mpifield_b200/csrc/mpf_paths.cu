@@ -52,21 +52,26 @@ static int run_deposit(PathArgs<T> a, const Tuning& t, cudaStream_t stream) {
             return run_deposit_private<T, NDIM, P, WHITNEY>(a, entries, stream);
     }
     if (t.path != 2) {
-        auto launch = [&](auto kernel, int threads) {
+        auto launch = [&](auto kernel, int threads, int smem = 0) {
             const int64_t blocks = std::min<int64_t>((a.n + threads - 1) / threads, (int64_t)sm_count() * 32);
-            kernel<<<(unsigned)std::max<int64_t>(blocks, 1), threads, 0, stream>>>(a);
+            kernel<<<(unsigned)std::max<int64_t>(blocks, 1), threads, smem, stream>>>(a);
         };
         // WHITNEY: five CTAs of 128 per SM (96 registers; 4% faster than two of 256 on a
         // sorted store). 128 registers a thread: two CTAs of 256 per SM for the spline edges
         // of degree <= 2 (no spills; QUADRATIC_EDGES 15% faster than one CTA; 96 or 80
         // registers spill and measured 15-25% slower), four of 128 for
         // the cubic edges (some spills, but twice the warps of one CTA of 256 at 178
-        // registers: CUBIC_EDGES 137 -> 97 ms at 2^25 paths). Variant 1: one CTA of 256;
+        // registers: CUBIC_EDGES 137 -> 97 ms at 2^25 paths), in 3D with the cross-axis weights
+        // of the Gauss points in shared memory, computed once per axis instead of once per edge
+        // along it (97 -> 86 ms; the same for degree 2 measured slower). Variant 1: one CTA of 256;
         // variant 3: spline paths a path at a time instead of piece by piece; variant 7:
         // never through private copies of a small field.
         if constexpr (!WHITNEY && P >= 3) {
             if (t.variant == 3) launch(deposit_paths_kernel<T, NDIM, P, WHITNEY, 256, 1, false>, 256);
             else if (t.variant == 1) launch(deposit_paths_kernel<T, NDIM, P, WHITNEY, 256, 1>, 256);
+            else if constexpr (NDIM == 3)
+                launch(deposit_paths_kernel<T, NDIM, P, WHITNEY, 128, 4, true, true>, 128,
+                       path_cache_bytes<T, NDIM, P>(128));
             else launch(deposit_paths_kernel<T, NDIM, P, WHITNEY, 128, 4>, 128);
         } else {
             if (t.variant == 1) launch(deposit_paths_kernel<T, NDIM, P, WHITNEY, 256, 1>, 256);

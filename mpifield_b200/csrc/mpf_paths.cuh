@@ -306,9 +306,13 @@ template <typename T> struct CutStream {
 
 // One piece of a spline path: q times the line integral of the edge functions from p0
 // to p0 + step (cell coordinates, clamped on bounded axes), added to the sink.
-template <typename T, int NDIM, int P, typename Sink>
+//
+// CS > 0: `cache` is this thread's column (stride CS) of a shared-memory table that holds,
+// for the axis being deposited, the weights of every Gauss point along the two axes across
+// it -- computed once per axis instead of once per edge along it.
+template <typename T, int NDIM, int P, typename Sink, int CS = 0>
 __device__ __forceinline__ void spline_piece(T q, const T* p0, const T* step, const Grid<T>& g, bool clamped,
-                                             const Sink& sink) {
+                                             const Sink& sink, T* cache = nullptr) {
     constexpr int NPTS = (P - 1 + (NDIM - 1) * P) / 2 + 1;
     if (!clamped) {
         // The Gauss points of a piece lie in one knot interval on every axis:
@@ -336,6 +340,20 @@ __device__ __forceinline__ void spline_piece(T q, const T* p0, const T* step, co
             // the axes across this one, in increasing order
             const int o1 = NDIM > 1 ? (axis == 0 ? 1 : 0) : 0;
             const int o2 = NDIM > 2 ? (axis == 2 ? 1 : 2) : 0;
+            if constexpr (CS > 0) {
+#pragma unroll
+                for (int gp = 0; gp < NPTS; ++gp) {
+                    const T off = Gauss<T, NPTS>::point(gp) - T(0.5);
+                    T wb[SX], wc[SX];
+                    uniform_weights<T, P>(st[o1] + off * step[o1], wb);
+                    uniform_weights<T, P>(st[o2] + off * step[o2], wc);
+#pragma unroll
+                    for (int b = 0; b < SX; ++b) {
+                        cache[(gp * 2 * SX + b) * CS] = wb[b];
+                        cache[(gp * 2 * SX + SX + b) * CS] = wc[b];
+                    }
+                }
+            }
             // one edge along the axis at a time: (P + 1)^(ndim - 1) sums
 #pragma unroll
             for (int e = 0; e < P; ++e) {
@@ -348,8 +366,16 @@ __device__ __forceinline__ void spline_piece(T q, const T* p0, const T* step, co
                     const T off = Gauss<T, NPTS>::point(gp) - T(0.5);
                     T wa[P > 0 ? P : 1], wb[SX], wc[SX];
                     uniform_weights<T, P - 1>(at[axis] + off * step[axis], wa);
-                    if constexpr (NDIM > 1) uniform_weights<T, P>(st[o1] + off * step[o1], wb);
-                    if constexpr (NDIM > 2) uniform_weights<T, P>(st[o2] + off * step[o2], wc);
+                    if constexpr (CS > 0) {
+#pragma unroll
+                        for (int b = 0; b < SX; ++b) {
+                            wb[b] = cache[(gp * 2 * SX + b) * CS];
+                            wc[b] = cache[(gp * 2 * SX + SX + b) * CS];
+                        }
+                    } else {
+                        if constexpr (NDIM > 1) uniform_weights<T, P>(st[o1] + off * step[o1], wb);
+                        if constexpr (NDIM > 2) uniform_weights<T, P>(st[o2] + off * step[o2], wc);
+                    }
                     const T along = q * Gauss<T, NPTS>::weight(gp) * step[axis] * wa[e];
 #pragma unroll
                     for (int b = 0; b < CB; ++b) {
@@ -786,8 +812,9 @@ __global__ void __launch_bounds__(256) deposit_paths_tiled_kernel(const PathArgs
 // the others deposit their next piece, so the lanes of a warp deposit pieces together
 // whatever the number of pieces of their paths (a loop over paths would hold every lane
 // until the warp's longest path is done). FLAT false: a path at a time.
-template <typename T, int NDIM, int P, bool WHITNEY, int STRIDE, bool FLAT, typename Sink>
-__device__ __forceinline__ void deposit_range(const PathArgs<T>& a, int64_t i, int64_t end, const Sink& sink) {
+template <typename T, int NDIM, int P, bool WHITNEY, int STRIDE, bool FLAT, typename Sink, int CS = 0>
+__device__ __forceinline__ void deposit_range(const PathArgs<T>& a, int64_t i, int64_t end, const Sink& sink,
+                                              T* cache = nullptr) {
     if constexpr (!WHITNEY && FLAT) {
         const bool clamped = any_clamped<T, NDIM>(a.g);
         SplineWalk<T, NDIM, P> walk;
@@ -805,7 +832,7 @@ __device__ __forceinline__ void deposit_range(const PathArgs<T>& a, int64_t i, i
                 walk.begin(r0, r1, a.g);
             }
             T p0[NDIM], step[NDIM];
-            if (walk.piece(a.g, p0, step)) spline_piece<T, NDIM, P>(q, p0, step, a.g, clamped, sink);
+            if (walk.piece(a.g, p0, step)) spline_piece<T, NDIM, P, Sink, CS>(q, p0, step, a.g, clamped, sink, cache);
             if (walk.ended) {
                 if (walk.more()) {  // a path of several stretches: its ends again
                     T r0[NDIM], r1[NDIM];
@@ -835,7 +862,8 @@ __device__ __forceinline__ void deposit_range(const PathArgs<T>& a, int64_t i, i
 // region of a sorted store). Lane l of warp w takes the path l * (BLOCK / 32) + w of
 // the BLOCK: the lanes of a warp are BLOCK / 32 paths apart, in different cells, so the
 // adds of one instruction do not pile onto the same edges.
-template <typename T, int NDIM, int P, bool WHITNEY, int BLOCK = 256, int MINB = 1, bool FLAT = true>
+template <typename T, int NDIM, int P, bool WHITNEY, int BLOCK = 256, int MINB = 1, bool FLAT = true,
+          bool CACHE = false>
 __global__ void __launch_bounds__(BLOCK, MINB) deposit_paths_kernel(const PathArgs<T> a) {
     GlobalEdgeSink<T, NDIM> sink;
     sink.edges = a.edges_out;
@@ -844,7 +872,21 @@ __global__ void __launch_bounds__(BLOCK, MINB) deposit_paths_kernel(const PathAr
     const int slot = (threadIdx.x & 31) * (BLOCK / 32) + (threadIdx.x >> 5);
     const int64_t per = ((a.n + gridDim.x - 1) / gridDim.x + BLOCK - 1) / BLOCK * BLOCK;
     const int64_t mine_end = min(a.n, (int64_t)(blockIdx.x + 1) * per);
-    deposit_range<T, NDIM, P, WHITNEY, BLOCK, FLAT>(a, (int64_t)blockIdx.x * per + slot, mine_end, sink);
+    if constexpr (CACHE) {
+        T* cache = reinterpret_cast<T*>(mpf_dynamic_smem) + threadIdx.x;
+        deposit_range<T, NDIM, P, WHITNEY, BLOCK, FLAT, GlobalEdgeSink<T, NDIM>, BLOCK>(
+            a, (int64_t)blockIdx.x * per + slot, mine_end, sink, cache);
+    } else {
+        deposit_range<T, NDIM, P, WHITNEY, BLOCK, FLAT>(a, (int64_t)blockIdx.x * per + slot, mine_end, sink);
+    }
+}
+
+// Shared memory of deposit_paths_kernel with CACHE: a column per thread of the cross-axis
+// weights of every Gauss point (two axes, P + 1 weights each).
+template <typename T, int NDIM, int P>
+constexpr int path_cache_bytes(int block) {
+    return (P - 1 + (NDIM - 1) * P) / 2 + 1 > 0 ? ((P - 1 + (NDIM - 1) * P) / 2 + 1) * 2 * (P + 1) * block * (int)sizeof(T)
+                                                 : 0;
 }
 
 // Adds v to edge (node per axis, axis) of a private copy of the whole edge field in
