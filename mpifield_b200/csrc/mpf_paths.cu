@@ -63,7 +63,8 @@ static int run_deposit(PathArgs<T> a, const Tuning& t, cudaStream_t stream) {
         // the cubic edges (some spills, but twice the warps of one CTA of 256 at 178
         // registers: CUBIC_EDGES 137 -> 97 ms at 2^25 paths), in 3D with the cross-axis weights
         // of the Gauss points in shared memory, computed once per axis instead of once per edge
-        // along it (97 -> 86 ms; the same for degree 2 measured slower). Variant 1: one CTA of 256;
+        // along it, and the points a rolled loop (97 -> 72 ms; the cache for degree 2 measured
+        // slower). Variant 1: one CTA of 256;
         // variant 3: spline paths a path at a time instead of piece by piece; variant 7:
         // never through private copies of a small field.
         if constexpr (!WHITNEY && P >= 3) {

@@ -226,8 +226,8 @@ template <typename T> struct Gauss<T, 3> {
 };
 template <typename T> struct Gauss<T, 4> {
     static __device__ __forceinline__ T point(int g) {
-        const T p[4] = {T(0.06943184420297371), T(0.33000947820757187), T(0.6699905217924281), T(0.9305681557970262)};
-        return p[g];
+        return g == 0 ? T(0.06943184420297371)
+                      : (g == 1 ? T(0.33000947820757187) : (g == 2 ? T(0.6699905217924281) : T(0.9305681557970262)));
     }
     static __device__ __forceinline__ T weight(int g) {
         return (g == 0 || g == 3) ? T(0.17392742256872692) : T(0.3260725774312731);
@@ -235,12 +235,13 @@ template <typename T> struct Gauss<T, 4> {
 };
 template <typename T> struct Gauss<T, 5> {
     static __device__ __forceinline__ T point(int g) {
-        const T p[5] = {T(0.04691007703066802), T(0.23076534494715845), T(0.5), T(0.7692346550528415), T(0.9530899229693319)};
-        return p[g];
+        return g == 0 ? T(0.04691007703066802)
+                      : (g == 1 ? T(0.23076534494715845)
+                                : (g == 2 ? T(0.5) : (g == 3 ? T(0.7692346550528415) : T(0.9530899229693319))));
     }
     static __device__ __forceinline__ T weight(int g) {
-        const T w[5] = {T(0.11846344252809454), T(0.2393143352496832), T(0.28444444444444444), T(0.2393143352496832), T(0.11846344252809454)};
-        return w[g];
+        return (g == 0 || g == 4) ? T(0.11846344252809454)
+                                  : ((g == 1 || g == 3) ? T(0.2393143352496832) : T(0.28444444444444444));
     }
 };
 
@@ -341,7 +342,7 @@ __device__ __forceinline__ void spline_piece(T q, const T* p0, const T* step, co
             const int o1 = NDIM > 1 ? (axis == 0 ? 1 : 0) : 0;
             const int o2 = NDIM > 2 ? (axis == 2 ? 1 : 2) : 0;
             if constexpr (CS > 0) {
-#pragma unroll
+#pragma unroll 1
                 for (int gp = 0; gp < NPTS; ++gp) {
                     const T off = Gauss<T, NPTS>::point(gp) - T(0.5);
                     T wb[SX], wc[SX];
@@ -361,7 +362,9 @@ __device__ __forceinline__ void spline_piece(T q, const T* p0, const T* step, co
                 T acc[CB * CC];
 #pragma unroll
                 for (int k = 0; k < CB * CC; ++k) acc[k] = T(0);
-#pragma unroll
+                // (with the cache the points are a loop, not unrolled: the unrolled cubic
+                // body outgrew the instruction cache)
+#pragma unroll ((CS > 0 || P >= 2) ? 1 : NPTS)
                 for (int gp = 0; gp < NPTS; ++gp) {
                     const T off = Gauss<T, NPTS>::point(gp) - T(0.5);
                     T wa[P > 0 ? P : 1], wb[SX], wc[SX];
