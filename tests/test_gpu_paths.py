@@ -141,7 +141,7 @@ def test_very_long_and_huge_paths_end():
         torch.cuda.synchronize()
 
 
-@pytest.mark.parametrize("degree", [1, 2])
+@pytest.mark.parametrize("degree", [1, 2, 3])
 def test_full_size_continuity_128_cubed(degree):
     """The path-deposit configuration: 128^3 periodic, 2^22 paths (of 2^25), |displacement| < 0.9 cell."""
     n = 1 << 22
