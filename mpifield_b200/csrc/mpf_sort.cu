@@ -3,8 +3,8 @@
 // The key of a marker is the tile of the anchor node of its stencil (mpf_stencil.cuh,
 // axis_anchor), row-major over the tiles; a marker whose values are all zero gets the
 // sentinel key num_tiles without its position being read. The sort is a least-
-// significant-digit radix sort of (key, marker) pairs with 8-bit digits, as many passes
-// as the key needs bits. Each pass: a per-CTA digit histogram, an exclusive scan of the
+// significant-digit radix sort of (key, marker) pairs with 8- to 10-bit digits, as few
+// passes as the key's bits allow. Each pass: a per-CTA digit histogram, an exclusive scan of the
 // histograms in digit-major order, and a stable scatter in which every warp ranks its
 // 32 keys of a round with __match_any_sync against a per-warp digit count, so the rank
 // of a key follows the marker order inside the warp, the warps of a CTA and the CTAs:
@@ -25,35 +25,56 @@ constexpr int kSortTile = kSortBlock * kSortItems;
 constexpr int kWarps = kSortBlock / 32;
 
 
+// The key of marker i at position x: its anchor node's tile, then (within) its cell.
 template <typename T, int NDIM, int KIND, int P>
-__global__ void tile_keys_kernel(const KeyArgs<T> a) {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.n;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        if (a.values) {
-            bool live = false;
-            for (int64_t c = 0; c < a.ncomp; ++c) live = live || a.values[c * a.val_stride + i] != T(0);
-            if (!live) {
-                a.keys[i] = a.sentinel;
-                continue;
+__device__ __forceinline__ void tile_key_of(const KeyArgs<T>& a, const T* x, int64_t i) {
+    int64_t key = 0, inner = 0;
+#pragma unroll
+    for (int d = 0; d < NDIM; ++d) {
+        const T rel = cells_from(x[d] - a.g.lower[d], a.g.cell[d], a.g.inv[d], a.g.pow2[d]);
+        const int anchor = axis_anchor<T, KIND, P>(rel, a.g.num[d], a.g.code[d]);
+        const int t = anchor / a.tile[d];
+        key = key * a.ntiles[d] + t;
+        inner = inner * a.tile[d] + (anchor - t * a.tile[d]);
+    }
+    if (a.within) {
+        int64_t cells = 1;
+#pragma unroll
+        for (int d = 0; d < NDIM; ++d) cells *= a.tile[d];
+        key = key * cells + inner;
+    }
+    a.keys[i] = (uint32_t)key;
+}
+
+// Four markers a thread per round (i, i + stride, ...), their positions loaded before any
+// key is formed, so a thread keeps 4 x NDIM loads in flight; four CTAs an SM, one wave.
+constexpr int kKeyUnroll = 4;
+constexpr int kKeyBlocksPerSm = 4;
+
+template <typename T, int NDIM, int KIND, int P>
+__global__ void __launch_bounds__(kSortBlock, kKeyBlocksPerSm) tile_keys_kernel(const KeyArgs<T> a) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i0 < a.n; i0 += stride * kKeyUnroll) {
+        bool live[kKeyUnroll];
+#pragma unroll
+        for (int u = 0; u < kKeyUnroll; ++u) {
+            const int64_t i = i0 + u * stride;
+            live[u] = i < a.n;
+            if (a.values && live[u]) {
+                bool any = false;
+                for (int64_t c = 0; c < a.ncomp; ++c) any = any || a.values[c * a.val_stride + i] != T(0);
+                if (!any) a.keys[i] = a.sentinel;
+                live[u] = any;
             }
         }
-        int64_t key = 0, inner = 0;
+        T x[kKeyUnroll][NDIM];
 #pragma unroll
-        for (int d = 0; d < NDIM; ++d) {
-            const T rel = cells_from(a.pos[d * a.pos_stride + i] - a.g.lower[d], a.g.cell[d], a.g.inv[d],
-                                     a.g.pow2[d]);
-            const int anchor = axis_anchor<T, KIND, P>(rel, a.g.num[d], a.g.code[d]);
-            const int t = anchor / a.tile[d];
-            key = key * a.ntiles[d] + t;
-            inner = inner * a.tile[d] + (anchor - t * a.tile[d]);
-        }
-        if (a.within) {
-            int64_t cells = 1;
+        for (int u = 0; u < kKeyUnroll; ++u)
 #pragma unroll
-            for (int d = 0; d < NDIM; ++d) cells *= a.tile[d];
-            key = key * cells + inner;
-        }
-        a.keys[i] = (uint32_t)key;
+            for (int d = 0; d < NDIM; ++d) x[u][d] = live[u] ? a.pos[d * a.pos_stride + i0 + u * stride] : T(0);
+#pragma unroll
+        for (int u = 0; u < kKeyUnroll; ++u)
+            if (live[u]) tile_key_of<T, NDIM, KIND, P>(a, x[u], i0 + u * stride);
     }
 }
 
@@ -150,15 +171,23 @@ __global__ void scan_chunks_kernel(uint32_t* data, int64_t count, const uint32_t
 // (__match_any_sync) against per-warp digit counts in shared memory. The tile's pairs are
 // then placed in shared memory in digit order (a CTA-wide scan of the digit counts) and
 // written out in that order: consecutive threads write consecutive ranks of one digit's
-// run, so the writes of a warp cover a few runs instead of 32 scattered words.
+// run, so the writes of a warp cover a few runs instead of 32 scattered words. The CTA's
+// output offsets of its digits are read once, at the start (two per thread), and folded
+// into the digit starts; a value is read where it is placed, not held through the ranking,
+// and the ranks are kept two to a register (64 registers: four CTAs an SM for digits of up
+// to 9 bits, against two when the values and ranks were held whole); a CTA past the
+// device-side count (a mover sort, its grid sized for every marker) returns at once.
 template <int BITS>
-__global__ void digit_scatter_kernel(const uint32_t* keys_in, const int32_t* vals_in, int64_t n,
-                                     const int64_t* n_dev, int shift, const uint32_t* offsets, int64_t nblocks,
-                                     uint32_t* keys_out, int32_t* vals_out) {
+__global__ void __launch_bounds__(kSortBlock, BITS <= 9 ? 4 : 3)
+    digit_scatter_kernel(const uint32_t* keys_in, const int32_t* vals_in, int64_t n, const int64_t* n_dev,
+                         int shift, const uint32_t* offsets, int64_t nblocks, uint32_t* keys_out,
+                         int32_t* vals_out) {
     constexpr int DIGITS = 1 << BITS;
     constexpr int PER = DIGITS / kSortBlock;  // digits a thread scans (DIGITS >= kSortBlock)
     static_assert(DIGITS % kSortBlock == 0, "a whole number of digits per thread");
     if (n_dev) n = min(n, *n_dev);
+    const int64_t base = (int64_t)blockIdx.x * kSortTile;
+    if (base >= n) return;  // the whole CTA: nothing of it is in the sort
     extern __shared__ uint32_t smem_words[];
     uint32_t* warp_count = smem_words;                 // [kWarps][DIGITS]
     uint32_t* digit_start = warp_count + kWarps * DIGITS;  // [DIGITS]: the tile's first place of a digit
@@ -167,27 +196,29 @@ __global__ void digit_scatter_kernel(const uint32_t* keys_in, const int32_t* val
     __shared__ uint32_t warp_sums[kWarps];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
+    uint32_t out_at[PER];  // this CTA's first output rank of each of the thread's digits
+#pragma unroll
+    for (int q = 0; q < PER; ++q) out_at[q] = offsets[(int64_t)(threadIdx.x * PER + q) * nblocks + blockIdx.x];
     for (int d = threadIdx.x; d < kWarps * DIGITS; d += blockDim.x) warp_count[d] = 0;
     __syncthreads();
     uint32_t* mine = warp_count + warp * DIGITS;
-    const int64_t base = (int64_t)blockIdx.x * kSortTile;
     const int64_t seg = base + (int64_t)warp * 32 * kSortItems;
     uint32_t key[kSortItems];
-    int32_t val[kSortItems];
-    uint32_t rank[kSortItems];
+    uint32_t rank[kSortItems / 2];  // two ranks (< kSortTile) per word
+    static_assert(kSortTile <= 65536 && kSortItems % 2 == 0, "ranks packed in halves");
     const unsigned below = (1u << lane) - 1u;
 #pragma unroll
     for (int r = 0; r < kSortItems; ++r) {
         const int64_t i = seg + (int64_t)r * 32 + lane;
         const bool have = i < n;
         key[r] = have ? keys_in[i] : 0xffffffffu;
-        val[r] = have ? (vals_in ? vals_in[i] : (int32_t)i) : 0;
         const uint32_t digit = (key[r] >> shift) & (DIGITS - 1);
         // lanes holding the same digit this round, and those of them before this lane
         const unsigned same = __match_any_sync(0xffffffffu, have ? (int)digit : -1 - lane);
         const unsigned before = __popc(same & below);
         const uint32_t count = have ? mine[digit] : 0;
-        rank[r] = count + before;
+        const uint32_t rk = count + before;
+        rank[r / 2] = (r & 1) ? (rank[r / 2] | (rk << 16)) : rk;
         __syncwarp();
         if (have && before == 0) mine[digit] = count + __popc(same);
         __syncwarp();
@@ -220,8 +251,10 @@ __global__ void digit_scatter_kernel(const uint32_t* keys_in, const int32_t* val
     uint32_t before_warps = 0;
     for (int w = 0; w < warp; ++w) before_warps += warp_sums[w];
     uint32_t at = before_warps + incl - run;
+    uint32_t start[PER];
 #pragma unroll
     for (int q = 0; q < PER; ++q) {
+        start[q] = at;
         digit_start[threadIdx.x * PER + q] = at;
         at += total[q];
     }
@@ -232,18 +265,20 @@ __global__ void digit_scatter_kernel(const uint32_t* keys_in, const int32_t* val
         const int64_t i = seg + (int64_t)r * 32 + lane;
         if (i < n) {
             const uint32_t digit = (key[r] >> shift) & (DIGITS - 1);
-            const uint32_t place = digit_start[digit] + mine[digit] + rank[r];
+            const uint32_t place = digit_start[digit] + mine[digit] + ((rank[r / 2] >> (16 * (r & 1))) & 0xffffu);
             tile_keys[place] = key[r];
-            tile_vals[place] = val[r];
+            tile_vals[place] = vals_in ? vals_in[i] : (int32_t)i;
         }
     }
     __syncthreads();
-    // written out in that order: place p of digit d goes to the digit's run of this CTA
-    const int count = (int)min((int64_t)kSortTile, max((int64_t)0, n - base));
+    // place p of digit d goes to rank out_at[d] + p - start[d] of the output
+#pragma unroll
+    for (int q = 0; q < PER; ++q) digit_start[threadIdx.x * PER + q] = out_at[q] - start[q];
+    __syncthreads();
+    const int count = (int)min((int64_t)kSortTile, n - base);
     for (int p = threadIdx.x; p < count; p += blockDim.x) {
         const uint32_t k = tile_keys[p];
-        const uint32_t digit = (k >> shift) & (DIGITS - 1);
-        const uint32_t dst = offsets[(int64_t)digit * nblocks + blockIdx.x] + (uint32_t)p - digit_start[digit];
+        const uint32_t dst = digit_start[(k >> shift) & (DIGITS - 1)] + (uint32_t)p;
         keys_out[dst] = k;
         vals_out[dst] = tile_vals[p];
     }
@@ -325,8 +360,9 @@ static int scan_exclusive(uint32_t* data, int64_t count, uint32_t* sums, cudaStr
 
 template <typename T, int NDIM, int KIND, int P>
 static int run_keys(const KeyArgs<T>& a, cudaStream_t stream) {
-    const int block = 256;
-    const int64_t blocks = std::min<int64_t>((a.n + block - 1) / block, (int64_t)sm_count() * 16);
+    const int block = kSortBlock;
+    const int64_t blocks = std::min<int64_t>((a.n + block * kKeyUnroll - 1) / (block * kKeyUnroll),
+                                             (int64_t)sm_count() * kKeyBlocksPerSm);
     tile_keys_kernel<T, NDIM, KIND, P><<<(unsigned)std::max<int64_t>(blocks, 1), block, 0, stream>>>(a);
     count_launches(1);
     return launch_status();
