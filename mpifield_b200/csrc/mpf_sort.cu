@@ -25,15 +25,17 @@ constexpr int kSortTile = kSortBlock * kSortItems;
 constexpr int kWarps = kSortBlock / 32;
 
 
-// The key of marker i at position x: its anchor node's tile, then (within) its cell.
+// The key of marker i at position x: its anchor node's tile, then (within) its cell. A
+// tile extent that is a power of two (shift[d] >= 0) divides a non-negative anchor by a
+// shift, the same quotient as the division.
 template <typename T, int NDIM, int KIND, int P>
-__device__ __forceinline__ void tile_key_of(const KeyArgs<T>& a, const T* x, int64_t i) {
+__device__ __forceinline__ void tile_key_of(const KeyArgs<T>& a, const T* x, int64_t i, const int* shift) {
     int64_t key = 0, inner = 0;
 #pragma unroll
     for (int d = 0; d < NDIM; ++d) {
         const T rel = cells_from(x[d] - a.g.lower[d], a.g.cell[d], a.g.inv[d], a.g.pow2[d]);
         const int anchor = axis_anchor<T, KIND, P>(rel, a.g.num[d], a.g.code[d]);
-        const int t = anchor / a.tile[d];
+        const int t = shift[d] >= 0 && anchor >= 0 ? anchor >> shift[d] : anchor / a.tile[d];
         key = key * a.ntiles[d] + t;
         inner = inner * a.tile[d] + (anchor - t * a.tile[d]);
     }
@@ -54,6 +56,9 @@ constexpr int kKeyBlocksPerSm = 4;
 template <typename T, int NDIM, int KIND, int P>
 __global__ void __launch_bounds__(kSortBlock, kKeyBlocksPerSm) tile_keys_kernel(const KeyArgs<T> a) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    int shift[NDIM];
+#pragma unroll
+    for (int d = 0; d < NDIM; ++d) shift[d] = (a.tile[d] & (a.tile[d] - 1)) == 0 ? __ffs(a.tile[d]) - 1 : -1;
     for (int64_t i0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i0 < a.n; i0 += stride * kKeyUnroll) {
         bool live[kKeyUnroll];
 #pragma unroll
@@ -74,7 +79,7 @@ __global__ void __launch_bounds__(kSortBlock, kKeyBlocksPerSm) tile_keys_kernel(
             for (int d = 0; d < NDIM; ++d) x[u][d] = live[u] ? a.pos[d * a.pos_stride + i0 + u * stride] : T(0);
 #pragma unroll
         for (int u = 0; u < kKeyUnroll; ++u)
-            if (live[u]) tile_key_of<T, NDIM, KIND, P>(a, x[u], i0 + u * stride);
+            if (live[u]) tile_key_of<T, NDIM, KIND, P>(a, x[u], i0 + u * stride, shift);
     }
 }
 

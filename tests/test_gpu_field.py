@@ -88,8 +88,8 @@ def test_tile_keys_and_order_are_bit_exact(kind, degree, ndim):
         geom, pos, _, values = random_case(rng, ndim, codes, degree, n=300_003, ncomp=2, shape=(37, 29, 23)[:ndim])
         values[:, ::5] = 0.0
         pos[:, ::10] = np.nan  # dead markers: keys without reading the position
-        tile = (8, 4, 2)[:ndim]
-        for within in (False, True):
+        # power-of-two extents (the key's quotient by a shift) and others (by a division)
+        for tile, within in ((ext[:ndim], w) for ext in ((8, 4, 2), (5, 3, 7)) for w in (False, True)):
             t = mf.sort_by_tile(cu(pos), (KIND_NAMES[kind], degree), geom, tile, cu(values), within=within)
             keys = O.tile_keys(kind, degree, pos, geom, tile, values, within=within)
             np.testing.assert_array_equal(t.keys.cpu().numpy().view(np.uint32), keys)
