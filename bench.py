@@ -69,6 +69,8 @@ def parse() -> argparse.Namespace:
     p.add_argument("--serve-requests", type=int, default=10000, help="requests of the serving stream (0: skip)")
     p.add_argument("--paths-only", type=int, default=0, metavar="N",
                    help="measure only the path deposits, at N paths on 128^3 (a profiling case)")
+    p.add_argument("--steady-only", action="store_true",
+                   help="measure only the steady step (push, re-sort, permute, gather, scatter; a profiling case)")
     p.add_argument("--autograd-only", action="store_true",
                    help="measure only the differentiation step (512^2 cubic, 2^22 markers; a profiling case)")
     p.add_argument("--serve-rate", type=float, default=20000.0,
@@ -425,10 +427,12 @@ def measure_steady(step, ps, ws, reps: int) -> dict:
 
     ms = _event_ms(one, reps)
     resort = []
+    torch.cuda.nvtx.range_push("steady")
     for _ in range(max(2, reps // 4)):
         one(ev)
         torch.cuda.synchronize()
         resort.append(ev[0].elapsed_time(ev[1]))
+    torch.cuda.nvtx.range_pop()
     # the last re-sort against a full sort of the same pushed store (spare[0]: the store
     # before the last permute)
     full = mf.sort_by_tile(spare[0], mf.QUADRATIC, step.geom, TILE, within=True)
@@ -1014,6 +1018,16 @@ def main() -> None:
                 peak, _ = read_peak()
                 print(json.dumps({"path_deposit": measure_paths(device, max(1, args.steps), peak, args.paths_only,
                                                                 cpu_sample=None)}))
+            return
+        if args.steady_only:
+            device = torch.device("cuda", local)
+            torch.cuda.set_device(device)
+            if rank == 0:
+                step = Step(args.markers, device, torch.float64)
+                pos, w = make_markers(args.markers, device, torch.float64, seed=1)
+                _, ps, ws = step.sort(pos, w)
+                del pos, w
+                print(json.dumps({"steady_step": measure_steady(step, ps, ws, max(2, args.steps))}))
             return
         if args.autograd_only:
             device = torch.device("cuda", local)
