@@ -92,10 +92,15 @@ __global__ void digit_histogram_kernel(const uint32_t* keys, int64_t n, const in
     for (int d = threadIdx.x; d < DIGITS; d += blockDim.x) hist[d] = 0;
     __syncthreads();
     const int64_t base = (int64_t)blockIdx.x * kSortTile;
-    for (int k = threadIdx.x; k < kSortTile; k += blockDim.x) {
-        const int64_t i = base + k;
-        if (i < n) atomicAdd(&hist[(keys[i] >> shift) & (DIGITS - 1)], 1u);
+    uint32_t key[kSortItems];  // the thread's keys loaded first, then counted
+#pragma unroll
+    for (int r = 0; r < kSortItems; ++r) {
+        const int64_t i = base + (int64_t)r * kSortBlock + threadIdx.x;
+        key[r] = i < n ? keys[i] : 0u;
     }
+#pragma unroll
+    for (int r = 0; r < kSortItems; ++r)
+        if (base + (int64_t)r * kSortBlock + threadIdx.x < n) atomicAdd(&hist[(key[r] >> shift) & (DIGITS - 1)], 1u);
     __syncthreads();
     for (int d = threadIdx.x; d < DIGITS; d += blockDim.x) counts[(int64_t)d * nblocks + blockIdx.x] = hist[d];
 }
@@ -212,11 +217,16 @@ __global__ void __launch_bounds__(kSortBlock, BITS <= 9 ? 4 : 3)
     uint32_t rank[kSortItems / 2];  // two ranks (< kSortTile) per word
     static_assert(kSortTile <= 65536 && kSortItems % 2 == 0, "ranks packed in halves");
     const unsigned below = (1u << lane) - 1u;
+    // all the segment's keys in flight at once, before the ranking's warp barriers
+#pragma unroll
+    for (int r = 0; r < kSortItems; ++r) {
+        const int64_t i = seg + (int64_t)r * 32 + lane;
+        key[r] = i < n ? keys_in[i] : 0xffffffffu;
+    }
 #pragma unroll
     for (int r = 0; r < kSortItems; ++r) {
         const int64_t i = seg + (int64_t)r * 32 + lane;
         const bool have = i < n;
-        key[r] = have ? keys_in[i] : 0xffffffffu;
         const uint32_t digit = (key[r] >> shift) & (DIGITS - 1);
         // lanes holding the same digit this round, and those of them before this lane
         const unsigned same = __match_any_sync(0xffffffffu, have ? (int)digit : -1 - lane);
@@ -528,12 +538,21 @@ __global__ void split_kernel(const uint32_t* knew, const uint32_t* kprev, int64_
     const int64_t base = (int64_t)blockIdx.x * kSortTile;
     if (threadIdx.x == 0) carry = 0;
     const uint32_t first_mover = offsets[blockIdx.x];
+    // the thread's keys of every round, new and previous, loaded before the rounds' barriers
+    uint32_t knew_r[kSortItems], kprev_r[kSortItems];
+#pragma unroll
+    for (int round = 0; round < kSortItems; ++round) {
+        const int64_t i = base + (int64_t)round * kSortBlock + threadIdx.x;
+        knew_r[round] = i < n ? knew[i] : 0;
+        kprev_r[round] = i < n ? kprev[i] : 0;
+    }
     __syncthreads();
+#pragma unroll
     for (int round = 0; round < kSortItems; ++round) {
         const int64_t i = base + (int64_t)round * kSortBlock + threadIdx.x;
         const bool have = i < n;
-        const uint32_t key = have ? knew[i] : 0;
-        const bool mover = have && key != kprev[i];
+        const uint32_t key = knew_r[round];
+        const bool mover = have && key != kprev_r[round];
         const unsigned ballot = __ballot_sync(0xffffffffu, mover);
         if (lane == 0) warp_movers[warp] = __popc(ballot);
         __syncthreads();
