@@ -25,6 +25,29 @@ constexpr int kSortTile = kSortBlock * kSortItems;
 constexpr int kWarps = kSortBlock / 32;
 
 
+// The rare cases of the key, out of line so that the key kernel's unrolled body keeps only
+// the usual case (inlined at every marker and axis, the wraps, clamps and divisions of the
+// rare ones outgrew the instruction cache).
+template <typename T, int KIND, int P>
+__device__ __noinline__ int axis_anchor_rare(T rel, int num, int code) {
+    return axis_anchor<T, KIND, P>(rel, num, code);
+}
+
+__device__ __noinline__ int quotient_rare(int a, int b) { return a / b; }
+
+// The anchor node of rel (axis_anchor). Usually the stencil's middle node `quick` lies in
+// [1, num - 2]: there every stencil takes it unchanged (no wrap, no clamp, no mapping), as
+// their own quick paths do, so it is the anchor; clamped spline axes of degree >= 1 and
+// everything else take the full computation.
+template <typename T, int KIND, int P>
+__device__ __forceinline__ int key_anchor(T rel, int num, int code) {
+    constexpr bool half = KIND == QUADRATIC || (KIND == SPLINE && P % 2 == 0);
+    const int quick = trunc_int<T>(half ? rel + T(0.5) : rel);
+    const bool clamped_spline = KIND == SPLINE && P >= 1 && code == CLAMPED;
+    if (quick >= 1 && quick <= num - 2 && !clamped_spline) return quick;
+    return axis_anchor_rare<T, KIND, P>(rel, num, code);
+}
+
 // The key of marker i at position x: its anchor node's tile, then (within) its cell. A
 // tile extent that is a power of two (shift[d] >= 0) divides a non-negative anchor by a
 // shift, the same quotient as the division.
@@ -34,8 +57,8 @@ __device__ __forceinline__ void tile_key_of(const KeyArgs<T>& a, const T* x, int
 #pragma unroll
     for (int d = 0; d < NDIM; ++d) {
         const T rel = cells_from(x[d] - a.g.lower[d], a.g.cell[d], a.g.inv[d], a.g.pow2[d]);
-        const int anchor = axis_anchor<T, KIND, P>(rel, a.g.num[d], a.g.code[d]);
-        const int t = shift[d] >= 0 && anchor >= 0 ? anchor >> shift[d] : anchor / a.tile[d];
+        const int anchor = key_anchor<T, KIND, P>(rel, a.g.num[d], a.g.code[d]);
+        const int t = shift[d] >= 0 && anchor >= 0 ? anchor >> shift[d] : quotient_rare(anchor, a.tile[d]);
         key = key * a.ntiles[d] + t;
         inner = inner * a.tile[d] + (anchor - t * a.tile[d]);
     }
